@@ -1,0 +1,195 @@
+"""Python interface of the B200 EZmock engine.
+
+``EZmock`` mirrors the reference's Cython wrapper (python/EZmock/EZmock.pyx,
+class EZmock at :36-485) method by method: same names, keyword arguments,
+defaults, and RuntimeError messages taken from EZmock_errmsg.  The wrapper is
+built in single precision in the reference (python/setup.py:56); here
+``prec=32`` (default) loads libEZmock_f32.so and ``prec=64`` libEZmock_f64.so.
+Catalogue arrays are returned as numpy arrays that own their memory.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["EZmock"]
+
+
+class EZmock:
+    def __init__(self, *args, prec=32, **kwargs):
+        """Lbox, Ngrid (required); rng (0: MRG32K3A, 1: MT19937, default 1);
+        seed (default 1); nthread (default 0)."""
+        if "Lbox" in kwargs:
+            Lbox = float(kwargs["Lbox"])
+        else:
+            raise KeyError("`Lbox` is a required argument")
+        if "Ngrid" in kwargs:
+            Ngrid = int(kwargs["Ngrid"])
+        else:
+            raise KeyError("`Ngrid` is a required argument")
+        rng = int(kwargs.get("rng", 1))
+        seed = int(kwargs.get("seed", 1))
+        nthread = int(kwargs.get("nthread", 0))
+        self._L = _lib.load(prec)
+        self._rdt = np.float32 if prec == 32 else np.float64
+        self._err = ctypes.c_int(0)
+        self._Ng = Ngrid
+        self._Lbox = Lbox
+        self._ez = self._L.EZmock_init(Lbox, Ngrid, rng, seed, nthread, ctypes.byref(self._err))
+        if not self._ez:
+            raise RuntimeError(self._L.EZmock_errmsg(self._err.value).decode("utf-8"))
+
+    def __del__(self):
+        ez = getattr(self, "_ez", None)
+        if ez:
+            self._L.EZmock_destroy(ez)
+            self._ez = None
+
+    def _assert_return_value(self):
+        if self._err.value != 0:
+            raise RuntimeError(self._L.EZmock_errmsg(self._err.value).decode("utf-8"))
+
+    # -- EZmock.pyx:113-133
+    def set_growth_params(self, growth_pk, vel_fac):
+        self._err.value = self._L.EZmock_set_cosmology(
+            self._ez, float(growth_pk), float(vel_fac), False, 0.0, 0.0, 0.0, 0.0, 0.0,
+            ctypes.byref(self._err))
+        self._assert_return_value()
+
+    # -- EZmock.pyx:136-158
+    def eval_growth_params(self, z_out, Omega_m, z_pk=0, Omega_nu=0, w=-1):
+        self._err.value = self._L.EZmock_set_cosmology(
+            self._ez, 0.0, 0.0, True, float(z_out), float(z_pk), float(Omega_m),
+            float(Omega_nu), float(w), ctypes.byref(self._err))
+        self._assert_return_value()
+
+    # -- EZmock.pyx:161-226
+    def setup_linear_pk(self, k, Plin, Pnw=None, BAO_enhance=0, interp_log=False):
+        try:
+            k = np.ascontiguousarray(np.asarray(k), dtype=np.float64)
+            Plin = np.ascontiguousarray(np.asarray(Plin), dtype=np.float64)
+        except Exception:
+            raise TypeError("`k` and `Plin` are expected to be float numpy arrays")
+        assert k.ndim == 1 and Plin.ndim == 1 and k.shape[0] == Plin.shape[0], \
+            "`k` and `Plin` must be 1d arrays with the same length"
+        if BAO_enhance != 0:
+            try:
+                Pnw = np.ascontiguousarray(np.asarray(Pnw), dtype=np.float64)
+            except Exception:
+                raise TypeError("`Pnw` is expected to be a float numpy array")
+            assert Pnw.ndim == 1 and k.shape[0] == Pnw.shape[0], \
+                "`Pnw` must be an 1d array with the same length as k"
+            pnw = Pnw.ctypes.data_as(ctypes.c_void_p)
+        else:
+            pnw = None
+        self._err.value = self._L.EZmock_setup_linear_pk(
+            self._ez, k.ctypes.data_as(ctypes.c_void_p), k.shape[0],
+            Plin.ctypes.data_as(ctypes.c_void_p), pnw, float(BAO_enhance),
+            bool(interp_log), ctypes.byref(self._err))
+        self._assert_return_value()
+
+    # -- EZmock.pyx:229-251
+    def create_dens_field_from_ic(self, fixamp=False, iphase=False):
+        self._err.value = self._L.EZmock_create_dens_field(
+            self._ez, None, False, None, bool(fixamp), bool(iphase), ctypes.byref(self._err))
+        self._assert_return_value()
+
+    # -- EZmock.pyx:254-283
+    def create_dens_field_from_wn(self, delta):
+        try:
+            delta = np.ascontiguousarray(np.asarray(delta), dtype=self._rdt)
+        except Exception:
+            raise TypeError("`delta` is expected to be a float numpy array")
+        assert delta.ndim == 1 and delta.shape[0] == self._Ng ** 3, \
+            f"`delta` must be a 1d array with {self._Ng:d}**3 elements"
+        self._err.value = self._L.EZmock_create_dens_field(
+            self._ez, None, False, delta.ctypes.data_as(ctypes.c_void_p), False, False,
+            ctypes.byref(self._err))
+        self._assert_return_value()
+
+    # -- EZmock.pyx:286-334
+    def create_dens_field_from_disp(self, dx, dy, dz, deepcopy=False):
+        try:
+            dx, dy, dz = (np.ascontiguousarray(np.asarray(a), dtype=self._rdt)
+                          for a in (dx, dy, dz))
+        except Exception:
+            raise TypeError("`dx`, `dy`, and `dz` must be float numpy arrays")
+        ntot = self._Ng ** 3
+        assert all(a.ndim == 1 and a.shape[0] == ntot for a in (dx, dy, dz)), \
+            f"`dx`, `dy`, `dz` must be 1d arrays with {self._Ng:d}**3 elements"
+        disp = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in (dx, dy, dz)])
+        self._err.value = self._L.EZmock_create_dens_field(
+            self._ez, ctypes.cast(disp, ctypes.c_void_p), bool(deepcopy), None, False, False,
+            ctypes.byref(self._err))
+        self._assert_return_value()
+
+    def _populate(self, rho_c, rho_exp, pdf_base, sigma_v, ntracer, att_part):
+        rt = self._L._rt
+        params = (rt * 4)(rho_c, rho_exp, pdf_base, sigma_v)
+        ptrs = [ctypes.POINTER(rt)() for _ in range(6)]
+        num = ctypes.c_size_t(0)
+        self._err.value = self._L.EZmock_populate_tracer(
+            self._ez, ctypes.cast(params, ctypes.c_void_p), int(ntracer), bool(att_part),
+            ctypes.byref(num), *[ctypes.byref(p) for p in ptrs], ctypes.byref(self._err))
+        self._assert_return_value()
+        return num.value, ptrs
+
+    # -- EZmock.pyx:337-405
+    def populate_tracer(self, rho_c, rho_exp, pdf_base, sigma_v, ntracer, att_part=False):
+        n, ptrs = self._populate(rho_c, rho_exp, pdf_base, sigma_v, ntracer, att_part)
+        libc = ctypes.CDLL(None)
+        libc.free.argtypes = [ctypes.c_void_p]
+        out = []
+        for p in ptrs:
+            arr = np.ctypeslib.as_array(p, shape=(n,)).copy() if n else np.zeros(0, self._rdt)
+            libc.free(ctypes.cast(p, ctypes.c_void_p))
+            out.append(arr)
+        return tuple(out)
+
+    # -- EZmock.pyx:408-485
+    def populate_tracer_to_file(self, rho_c, rho_exp, pdf_base, sigma_v, ntracer, fname,
+                                att_part=False, rsd_fac=0, header=True):
+        n, ptrs = self._populate(rho_c, rho_exp, pdf_base, sigma_v, ntracer, att_part)
+        self._err.value = self._L.EZmock_write_ascii(
+            self._ez, *ptrs, n, float(rsd_fac), bool(header), str(fname).encode("utf-8"),
+            ctypes.byref(self._err))
+        libc = ctypes.CDLL(None)
+        libc.free.argtypes = [ctypes.c_void_p]
+        for p in ptrs:
+            libc.free(ctypes.cast(p, ctypes.c_void_p))
+        self._assert_return_value()
+
+    # ---- extensions (no counterpart in the reference wrapper) ----
+    def set_option(self, option, value):
+        self._err.value = self._L.EZmockB200_set_option(self._ez, int(option), int(value),
+                                                        ctypes.byref(self._err))
+        self._assert_return_value()
+
+    def field(self, which):
+        """Copy of a device field: 0..2 psi, 3 rho, 4..6 painted displacements."""
+        out = np.empty(self._Ng ** 3, self._rdt)
+        self._err.value = self._L.EZmockB200_copy_field(
+            self._ez, int(which), out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(self._err))
+        self._assert_return_value()
+        return out.reshape((self._Ng,) * 3)
+
+    def stage_times(self):
+        ms = (ctypes.c_double * 11)()
+        n = self._L.EZmockB200_stage_times(self._ez, ms, 11)
+        names = ["rng", "ic", "fft_i", "fft_j", "fft_k", "cic", "bias", "select", "emit",
+                 "vel", "d2h"]
+        return {names[i]: ms[i] for i in range(n)}
+
+    def populate_device(self, rho_c, rho_exp, pdf_base, sigma_v, ntracer):
+        rt = self._L._rt
+        params = (rt * 4)(rho_c, rho_exp, pdf_base, sigma_v)
+        num = ctypes.c_size_t(0)
+        self._err.value = self._L.EZmockB200_populate_device(
+            self._ez, ctypes.cast(params, ctypes.c_void_p), int(ntracer), ctypes.byref(num),
+            ctypes.byref(self._err))
+        self._assert_return_value()
+        return num.value
+
+    def sync(self):
+        return self._L.EZmockB200_sync(self._ez)

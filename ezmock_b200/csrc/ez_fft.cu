@@ -1,0 +1,519 @@
+// ez_fft.cu -- the three Zel'dovich displacement fields by 3D complex-to-real
+// FFTs (libEZmock/EZmock/perturb.c:361-398, FFTW plans at dens_field.c:141).
+//
+// psi_d = c2r(S * k_d) for d = x, y, z, with S the initial Fourier field and
+// k_x = freq(i), k_y = freq(j), k_z = k.  The transform follows FFTW's
+// multi-dimensional real-data convention: complex (backward, unnormalised)
+// transforms over the i and j axes, then a 1D complex-to-real transform
+// along k that ignores the imaginary parts of the k = 0 and k = Ng/2 terms.
+// The reference's kz = 0 / Nyquist planes are not Hermitian, so the order
+// matters and is kept.
+//
+// Three HBM passes, each a batch of 1D transforms staged through shared
+// memory (Stockham autosort, radices 8/4/2/3/5, twiddles rounded from long
+// double on the host):
+//   pass I : tiles [all i] x [K columns of k] for one j.  Because k_y and k_z
+//            are constant along i, only two transforms are needed:
+//            A_x = FFT_i(S k_x), A_0 = FFT_i(S).
+//   pass J : tiles [all j] x [K columns] for one x.
+//            B_x = FFT_j(A_x), B_y = FFT_j(A_0 k_y), B_0 = FFT_j(A_0).
+//   pass K : per (x, y) row, c2r of B_x, B_y and k B_0 through a half-length
+//            complex FFT (even/odd packing), written as psi rows.
+// Traffic: S read once; 2 + 3 spectra written, 5 read; 3 real fields written.
+#include "ez_internal.cuh"
+
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <vector>
+
+typedef decltype(cplx::x) rt;
+
+namespace {
+
+constexpr int FFT_NT = 512;       // threads per block
+constexpr int MAXF = 12;
+
+struct FftPlanDev {
+  int n, nfac;
+  int fac[MAXF];
+  const cplx *tw;                  // tw[e] = exp(+2 pi i e / n)
+};
+
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+  cplx c;
+  c.x = a.x * b.x - a.y * b.y;
+  c.y = a.x * b.y + a.y * b.x;
+  return c;
+}
+__device__ __forceinline__ cplx cadd(cplx a, cplx b) { cplx c; c.x = a.x + b.x; c.y = a.y + b.y; return c; }
+__device__ __forceinline__ cplx csub(cplx a, cplx b) { cplx c; c.x = a.x - b.x; c.y = a.y - b.y; return c; }
+// multiply by s*i
+__device__ __forceinline__ cplx cmuli(cplx a, int s) { cplx c; c.x = -s * a.y; c.y = s * a.x; return c; }
+
+template <int S>
+__device__ __forceinline__ void dft2(cplx *u) {
+  const cplx a = u[0], b = u[1];
+  u[0] = cadd(a, b); u[1] = csub(a, b);
+}
+
+template <int S>
+__device__ __forceinline__ void dft4(cplx *u) {
+  const cplx t0 = cadd(u[0], u[2]), t1 = csub(u[0], u[2]);
+  const cplx t2 = cadd(u[1], u[3]), t3 = cmuli(csub(u[1], u[3]), S);
+  u[0] = cadd(t0, t2); u[2] = csub(t0, t2);
+  u[1] = cadd(t1, t3); u[3] = csub(t1, t3);
+}
+
+template <int S>
+__device__ __forceinline__ void dft8(cplx *u) {
+  cplx a[4] = {u[0], u[2], u[4], u[6]}, b[4] = {u[1], u[3], u[5], u[7]};
+  dft4<S>(a);
+  dft4<S>(b);
+  const rt h = (rt) 0.70710678118654752440084436210484904;
+  // w8^k = exp(S i pi k / 4)
+  cplx w1; w1.x = h; w1.y = S * h;
+  cplx w3; w3.x = -h; w3.y = S * h;
+  b[1] = cmul(b[1], w1);
+  b[2] = cmuli(b[2], S);
+  b[3] = cmul(b[3], w3);
+#pragma unroll
+  for (int k = 0; k < 4; k++) { u[k] = cadd(a[k], b[k]); u[k + 4] = csub(a[k], b[k]); }
+}
+
+template <int S>
+__device__ __forceinline__ void dft3(cplx *u) {
+  const rt c = (rt) -0.5, sn = (rt) (S * 0.86602540378443864676372317075293618);
+  const cplx s12 = cadd(u[1], u[2]), d12 = csub(u[1], u[2]);
+  cplx t; t.x = u[0].x + c * s12.x; t.y = u[0].y + c * s12.y;
+  cplx v; v.x = -sn * d12.y; v.y = sn * d12.x;        // i * sn * d12
+  u[0] = cadd(u[0], s12);
+  u[1] = cadd(t, v);
+  u[2] = csub(t, v);
+}
+
+template <int S>
+__device__ __forceinline__ void dft5(cplx *u) {
+  const rt c1 = (rt) 0.30901699437494742410229341718281906;
+  const rt c2 = (rt) -0.80901699437494742410229341718281906;
+  const rt s1 = (rt) (S * 0.95105651629515357211643933337938214);
+  const rt s2 = (rt) (S * 0.58778525229247312916870595463907277);
+  const cplx a14 = cadd(u[1], u[4]), d14 = csub(u[1], u[4]);
+  const cplx a23 = cadd(u[2], u[3]), d23 = csub(u[2], u[3]);
+  cplx t1, t2, v1, v2;
+  t1.x = u[0].x + c1 * a14.x + c2 * a23.x; t1.y = u[0].y + c1 * a14.y + c2 * a23.y;
+  t2.x = u[0].x + c2 * a14.x + c1 * a23.x; t2.y = u[0].y + c2 * a14.y + c1 * a23.y;
+  // v1 = i (s1 d14 + s2 d23), v2 = i (s2 d14 - s1 d23)
+  const rt w1r = s1 * d14.x + s2 * d23.x, w1i = s1 * d14.y + s2 * d23.y;
+  const rt w2r = s2 * d14.x - s1 * d23.x, w2i = s2 * d14.y - s1 * d23.y;
+  v1.x = -w1i; v1.y = w1r;
+  v2.x = -w2i; v2.y = w2r;
+  u[0] = cadd(u[0], cadd(a14, a23));
+  u[1] = cadd(t1, v1);
+  u[4] = csub(t1, v1);
+  u[2] = cadd(t2, v2);
+  u[3] = csub(t2, v2);
+}
+
+// One Stockham pass of radix R over `nlines` lines of length n:
+// element e of line L is at buf[e*es + L].  Out of place (src -> dst).
+template <int R, int S>
+__device__ __forceinline__ void stockham_pass(const cplx *src, cplx *dst,
+    int n, int nlines, int es, int p, const cplx *tw) {
+  const int T = n / R;
+  const int nb = T * nlines;
+  const int stw = n / (p * R);
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    const int L = b % nlines, i = b / nlines;
+    const int k = i % p;
+    cplx u[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      cplx v = src[(i + q * T) * es + L];
+      if (q && k) {
+        const int e = (q * k * stw) % n;
+        cplx w = tw[e];
+        if (S < 0) w.y = -w.y;
+        v = cmul(v, w);
+      }
+      u[q] = v;
+    }
+    if (R == 2) dft2<S>(u);
+    else if (R == 3) dft3<S>(u);
+    else if (R == 4) dft4<S>(u);
+    else if (R == 5) dft5<S>(u);
+    else dft8<S>(u);
+    const int j = (i - k) * R + k;
+#pragma unroll
+    for (int s = 0; s < R; s++) dst[(j + s * p) * es + L] = u[s];
+  }
+}
+
+// Batched FFT of `nlines` lines held in a (element-major, line-minor) layout;
+// ping-pongs between a and b, returns the buffer holding the result.
+template <int S>
+__device__ cplx *smem_fft(cplx *a, cplx *b, int nlines, const FftPlanDev &pl,
+    const cplx *tw) {
+  int p = 1;
+  cplx *src = a, *dst = b;
+  for (int f = 0; f < pl.nfac; f++) {
+    const int r = pl.fac[f];
+    switch (r) {
+      case 8: stockham_pass<8, S>(src, dst, pl.n, nlines, nlines, p, tw); break;
+      case 4: stockham_pass<4, S>(src, dst, pl.n, nlines, nlines, p, tw); break;
+      case 2: stockham_pass<2, S>(src, dst, pl.n, nlines, nlines, p, tw); break;
+      case 3: stockham_pass<3, S>(src, dst, pl.n, nlines, nlines, p, tw); break;
+      default: stockham_pass<5, S>(src, dst, pl.n, nlines, nlines, p, tw); break;
+    }
+    __syncthreads();
+    p *= r;
+    cplx *t = src; src = dst; dst = t;
+  }
+  return src;
+}
+
+__device__ __forceinline__ rt freq_of(int i, int Ng) {
+  return (rt) ((i <= (Ng >> 1)) ? i : i - Ng);
+}
+
+// ---------------------------------------------------------------- pass I --
+__global__ void __launch_bounds__(FFT_NT)
+fft_pass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax,
+    cplx *__restrict__ A0, int Ng, int Nkp, int K, FftPlanDev pl) {
+  extern __shared__ unsigned char smraw[];
+  cplx *tw = (cplx *) smraw;
+  const int nl = 2 * K;
+  cplx *ba = tw + Ng;
+  cplx *bb = ba + (size_t) Ng * nl;
+  const int j = blockIdx.x, k0 = blockIdx.y * K;
+  for (int e = threadIdx.x; e < Ng; e += blockDim.x) tw[e] = pl.tw[e];
+  const size_t pstride = (size_t) Ng * Nkp;           // stride between i planes
+  for (int e = threadIdx.x; e < Ng * K; e += blockDim.x) {
+    const int i = e / K, c = e - i * K;
+    const cplx v = S[i * pstride + (size_t) j * Nkp + k0 + c];
+    const rt f = freq_of(i, Ng);
+    cplx w; w.x = v.x * f; w.y = v.y * f;
+    ba[i * nl + c] = w;
+    ba[i * nl + K + c] = v;
+  }
+  __syncthreads();
+  cplx *res = smem_fft<1>(ba, bb, nl, pl, tw);
+  for (int e = threadIdx.x; e < Ng * K; e += blockDim.x) {
+    const int i = e / K, c = e - i * K;
+    const size_t g = i * pstride + (size_t) j * Nkp + k0 + c;
+    Ax[g] = res[i * nl + c];
+    A0[g] = res[i * nl + K + c];
+  }
+}
+
+// ---------------------------------------------------------------- pass J --
+// In: Ax (spec1), A0 (spec2).  Out: Bx -> spec1, By -> spec0, B0 -> spec2.
+__global__ void __launch_bounds__(FFT_NT)
+fft_pass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
+    int Ng, int Nkp, int K, FftPlanDev pl) {
+  extern __shared__ unsigned char smraw[];
+  cplx *tw = (cplx *) smraw;
+  const int nl = 3 * K;
+  cplx *ba = tw + Ng;
+  cplx *bb = ba + (size_t) Ng * nl;
+  const int x = blockIdx.x, k0 = blockIdx.y * K;
+  for (int e = threadIdx.x; e < Ng; e += blockDim.x) tw[e] = pl.tw[e];
+  const size_t base = (size_t) x * Ng * Nkp + k0;
+  for (int e = threadIdx.x; e < Ng * K; e += blockDim.x) {
+    const int j = e / K, c = e - j * K;
+    const size_t g = base + (size_t) j * Nkp + c;
+    const cplx ax = s1[g], a0 = s2[g];
+    const rt f = freq_of(j, Ng);
+    cplx w; w.x = a0.x * f; w.y = a0.y * f;
+    ba[j * nl + c] = ax;
+    ba[j * nl + K + c] = w;
+    ba[j * nl + 2 * K + c] = a0;
+  }
+  __syncthreads();
+  cplx *res = smem_fft<1>(ba, bb, nl, pl, tw);
+  for (int e = threadIdx.x; e < Ng * K; e += blockDim.x) {
+    const int j = e / K, c = e - j * K;
+    const size_t g = base + (size_t) j * Nkp + c;
+    s1[g] = res[j * nl + c];
+    s0[g] = res[j * nl + K + c];
+    s2[g] = res[j * nl + 2 * K + c];
+  }
+}
+
+// ---------------------------------------------------------------- pass K --
+// R rows per block; lines: (row, component) with component 0: Bx -> psi0,
+// 1: By -> psi1, 2: k*B0 -> psi2.
+__global__ void __launch_bounds__(FFT_NT)
+fft_pass_k(const cplx *__restrict__ s0, const cplx *__restrict__ s1,
+    const cplx *__restrict__ s2, real *__restrict__ p0, real *__restrict__ p1,
+    real *__restrict__ p2, int Ng, int Nkp, int R, size_t nrows,
+    FftPlanDev pl, const cplx *__restrict__ twg) {
+  extern __shared__ unsigned char smraw[];
+  const int Nh = Ng >> 1;
+  const int nl = 3 * R;
+  cplx *tw = (cplx *) smraw;            // Nh
+  cplx *tg = tw + Nh;                   // Nh: exp(+2 pi i k / Ng)
+  cplx *raw = tg + Nh;                  // nl x (Nh+1), line-major
+  cplx *ba = raw + (size_t) nl * (Nh + 1);
+  cplx *bb = ba + (size_t) Nh * nl;
+  for (int e = threadIdx.x; e < Nh; e += blockDim.x) { tw[e] = pl.tw[e]; tg[e] = twg[e]; }
+  const size_t row0 = (size_t) blockIdx.x * R;
+  // load rows (only k <= Nh is needed)
+  for (int e = threadIdx.x; e < nl * (Nh + 1); e += blockDim.x) {
+    const int L = e / (Nh + 1), k = e - L * (Nh + 1);
+    const int r = L / 3, comp = L - 3 * r;
+    const size_t row = row0 + r;
+    cplx v; v.x = 0; v.y = 0;
+    if (row < nrows) {
+      const size_t g = row * Nkp + k;
+      if (comp == 0) v = s1[g];
+      else if (comp == 1) v = s0[g];
+      else { v = s2[g]; v.x *= (rt) k; v.y *= (rt) k; }
+    }
+    raw[e] = v;
+  }
+  __syncthreads();
+  // even/odd packing: Z[k] = E[k] + i O[k]
+  for (int e = threadIdx.x; e < nl * Nh; e += blockDim.x) {
+    const int L = e % nl, k = e / nl;
+    const cplx *X = raw + (size_t) L * (Nh + 1);
+    const rt xr = X[k].x, xi = (k == 0) ? (rt) 0 : X[k].y;
+    const rt yr = X[Nh - k].x, yi = (k == 0) ? (rt) 0 : -X[Nh - k].y;
+    const rt er = xr + yr, ei = xi + yi;
+    const rt dr = xr - yr, di = xi - yi;
+    const cplx w = tg[k];
+    const rt orr = dr * w.x - di * w.y, oi = dr * w.y + di * w.x;
+    cplx z; z.x = er - oi; z.y = ei + orr;
+    ba[k * nl + L] = z;
+  }
+  __syncthreads();
+  cplx *res = smem_fft<1>(ba, bb, nl, pl, tw);
+  for (int e = threadIdx.x; e < nl * Nh; e += blockDim.x) {
+    const int L = e / Nh, m = e - L * Nh;
+    const int r = L / 3, comp = L - 3 * r;
+    const size_t row = row0 + r;
+    if (row >= nrows) continue;
+    real *dst = (comp == 0) ? p0 : (comp == 1) ? p1 : p2;
+    const cplx z = res[m * nl + L];
+    cplx *d2 = (cplx *) (dst + row * Ng);
+    d2[m] = z;
+  }
+}
+
+// ------------------------------------------- forward transforms (r2c) ---
+// Row r2c along k (sign -1): even/odd packing into a half-length complex FFT,
+// then X[k] = E[k] + exp(-2 pi i k/Ng) O[k] for k = 0..Ng/2.
+__global__ void __launch_bounds__(FFT_NT)
+fft_r2c_rows(const real *__restrict__ x, cplx *__restrict__ S, int Ng,
+    int Nkp, int R, size_t nrows, FftPlanDev pl, const cplx *__restrict__ twg) {
+  extern __shared__ unsigned char smraw[];
+  const int Nh = Ng >> 1;
+  cplx *tw = (cplx *) smraw;
+  cplx *tg = tw + Nh;                   // Nh + 1 entries
+  cplx *ba = tg + Nh + 1;
+  cplx *bb = ba + (size_t) Nh * R;
+  for (int e = threadIdx.x; e < Nh; e += blockDim.x) tw[e] = pl.tw[e];
+  for (int e = threadIdx.x; e <= Nh; e += blockDim.x) tg[e] = twg[e];
+  const size_t row0 = (size_t) blockIdx.x * R;
+  for (int e = threadIdx.x; e < R * Nh; e += blockDim.x) {
+    const int r = e / Nh, mm = e - r * Nh;
+    cplx v; v.x = 0; v.y = 0;
+    if (row0 + r < nrows) v = ((const cplx *) (x + (row0 + r) * Ng))[mm];
+    ba[mm * R + r] = v;
+  }
+  __syncthreads();
+  cplx *Z = smem_fft<-1>(ba, bb, R, pl, tw);
+  for (int e = threadIdx.x; e < R * Nkp; e += blockDim.x) {
+    const int r = e / Nkp, k = e - r * Nkp;
+    const size_t row = row0 + r;
+    if (row >= nrows) continue;
+    cplx out; out.x = 0; out.y = 0;
+    if (k <= Nh) {
+      const int k1 = k % Nh, k2 = (Nh - k) % Nh;
+      const cplx a = Z[k1 * R + r], b = Z[k2 * R + r];
+      const rt er = (rt) 0.5 * (a.x + b.x), ei = (rt) 0.5 * (a.y - b.y);
+      const rt dr = (rt) 0.5 * (a.x - b.x), di = (rt) 0.5 * (a.y + b.y);
+      const rt orr = di, oi = -dr;                 // O = (Z - conj)/(2i)
+      const cplx w = tg[k];
+      const rt c = w.x, s = -w.y;                  // exp(-2 pi i k / Ng)
+      out.x = er + orr * c - oi * s;
+      out.y = ei + orr * s + oi * c;
+    }
+    S[row * Nkp + k] = out;
+  }
+}
+
+// In-place complex transform of one spectrum along axis 0 (i) or 1 (j).
+template <int S>
+__global__ void __launch_bounds__(FFT_NT)
+fft_axis_one(cplx *__restrict__ a, int Ng, int Nkp, int K, int axis,
+    FftPlanDev pl) {
+  extern __shared__ unsigned char smraw[];
+  cplx *tw = (cplx *) smraw;
+  cplx *ba = tw + Ng;
+  cplx *bb = ba + (size_t) Ng * K;
+  const int o = blockIdx.x, k0 = blockIdx.y * K;
+  for (int e = threadIdx.x; e < Ng; e += blockDim.x) tw[e] = pl.tw[e];
+  const size_t stride = axis == 0 ? (size_t) Ng * Nkp : (size_t) Nkp;
+  const size_t base = axis == 0 ? (size_t) o * Nkp + k0 : (size_t) o * Ng * Nkp + k0;
+  for (int e = threadIdx.x; e < Ng * K; e += blockDim.x) {
+    const int i = e / K, c = e - i * K;
+    ba[i * K + c] = a[base + i * stride + c];
+  }
+  __syncthreads();
+  cplx *res = smem_fft<S>(ba, bb, K, pl, tw);
+  for (int e = threadIdx.x; e < Ng * K; e += blockDim.x) {
+    const int i = e / K, c = e - i * K;
+    a[base + i * stride + c] = res[i * K + c];
+  }
+}
+
+__global__ void scale_kernel(real *a, size_t n, real f) {
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t) gridDim.x * blockDim.x)
+    a[i] *= f;
+}
+
+// --------------------------------------------------------------- host side
+struct TwTable {
+  cplx *dev = nullptr;
+  int n = 0;
+};
+std::mutex g_tw_mu;
+std::map<std::pair<int, int>, cplx *> g_tw;       // (device, n) -> table
+
+cplx *twiddles(int dev, int n) {
+  std::lock_guard<std::mutex> lk(g_tw_mu);
+  auto key = std::make_pair(dev, n);
+  auto it = g_tw.find(key);
+  if (it != g_tw.end()) return it->second;
+  std::vector<cplx> h(n);
+  const long double tpi = 6.283185307179586476925286766559005768L;
+  for (int e = 0; e < n; e++) {
+    const long double a = tpi * (long double) e / (long double) n;
+    h[e].x = (rt) cosl(a);
+    h[e].y = (rt) sinl(a);
+  }
+  cplx *d = nullptr;
+  if (!EZ_CUDA_OK(cudaMalloc(&d, sizeof(cplx) * n)) ||
+      !EZ_CUDA_OK(cudaMemcpy(d, h.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice)))
+    return nullptr;
+  g_tw[key] = d;
+  return d;
+}
+
+bool make_plan(int dev, int n, FftPlanDev *pl) {
+  pl->n = n;
+  pl->nfac = 0;
+  int m = n;
+  while (m > 1) {
+    int r = 0;
+    if (m % 8 == 0) r = 8;
+    else if (m % 4 == 0) r = 4;
+    else if (m % 2 == 0) r = 2;
+    else if (m % 3 == 0) r = 3;
+    else if (m % 5 == 0) r = 5;
+    else return false;
+    if (pl->nfac >= MAXF) return false;
+    pl->fac[pl->nfac++] = r;
+    m /= r;
+  }
+  pl->tw = twiddles(dev, n);
+  return pl->tw != nullptr;
+}
+
+}  // namespace
+
+// Columns per tile for passes I and J: 3 K Ng complex values per buffer stay
+// within the shared-memory budget (two ping-pong buffers per block).
+int ez_fft_tile_k(int Ng) {
+  int K = 16;
+  while (K > 1 && (size_t) 3 * K * Ng * sizeof(cplx) > 96 * 1024) K >>= 1;
+  return K;
+}
+
+// Grid sizes the GPU transforms handle: even, 5-smooth, and small enough that
+// one column (pass J, K = 1) and one row (pass K, R = 1) fit shared memory.
+bool ez_fft_supported(int Ng) {
+  if (Ng < 8 || (Ng & 1)) return false;
+  int m = Ng;
+  for (int r : {2, 3, 5}) while (m % r == 0) m /= r;
+  if (m != 1) return false;
+  const size_t Nh = Ng / 2;
+  const size_t sm_j = sizeof(cplx) * ((size_t) Ng + 2 * (size_t) Ng * 3);
+  const size_t sm_k = sizeof(cplx) * (2 * Nh + 3 * (Nh + 1) + 2 * Nh * 3);
+  return sm_j <= 200 * 1024 && sm_k <= 200 * 1024;
+}
+
+int ez_fft_c2r_psi(EzMesh *m) {
+  const int Ng = m->Ng, Nkp = m->Nkp, Nh = Ng / 2;
+  const int K = ez_fft_tile_k(Ng);
+  FftPlanDev pn, ph;
+  if (!make_plan(m->device, Ng, &pn) || !make_plan(m->device, Nh, &ph))
+    return EZMOCK_ERR_UNKNOWN;
+  const cplx *twg = twiddles(m->device, Ng);
+  if (!twg) return EZMOCK_ERR_UNKNOWN;
+
+  const size_t sm_i = sizeof(cplx) * ((size_t) Ng + 2 * (size_t) Ng * 2 * K);
+  const size_t sm_j = sizeof(cplx) * ((size_t) Ng + 2 * (size_t) Ng * 3 * K);
+  int R = 4;
+  while (R > 1 && sizeof(cplx) * (2 * (size_t) Nh + 3 * R * (Nh + 1) + 2 * (size_t) Nh * 3 * R) > 160 * 1024) R >>= 1;
+  const size_t sm_k = sizeof(cplx) * (2 * (size_t) Nh + 3 * R * (size_t) (Nh + 1) + 2 * (size_t) Nh * 3 * R);
+  static int attr_done = 0;
+  if (!attr_done) {
+    cudaFuncSetAttribute(fft_pass_i, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(fft_pass_j, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(fft_pass_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done = 1;
+  }
+  const int nkt = (m->Nk + K - 1) / K;
+  ez_stage_begin(m, ST_FFT_I);
+  fft_pass_i<<<dim3(Ng, nkt), FFT_NT, sm_i, m->stream>>>(m->spec[0], m->spec[1],
+      m->spec[2], Ng, Nkp, K, pn);
+  ez_stage_end(m, ST_FFT_I);
+  ez_stage_begin(m, ST_FFT_J);
+  fft_pass_j<<<dim3(Ng, nkt), FFT_NT, sm_j, m->stream>>>(m->spec[0], m->spec[1],
+      m->spec[2], Ng, Nkp, K, pn);
+  ez_stage_end(m, ST_FFT_J);
+  const size_t nrows = (size_t) Ng * Ng;
+  ez_stage_begin(m, ST_FFT_K);
+  fft_pass_k<<<(unsigned) ((nrows + R - 1) / R), FFT_NT, sm_k, m->stream>>>(
+      m->spec[0], m->spec[1], m->spec[2], m->psi[0], m->psi[1], m->psi[2], Ng,
+      Nkp, R, nrows, ph, twg);
+  ez_stage_end(m, ST_FFT_K);
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+// r2c(delta) (sign -1, unnormalised) into spec[0]
+// (libEZmock/EZmock/dens_field.c:195-201).
+int ez_fft_r2c_delta(EzMesh *m, const real *d_delta) {
+  const int Ng = m->Ng, Nkp = m->Nkp, Nh = Ng / 2;
+  FftPlanDev pn, ph;
+  if (!make_plan(m->device, Ng, &pn) || !make_plan(m->device, Nh, &ph))
+    return EZMOCK_ERR_UNKNOWN;
+  const cplx *twg = twiddles(m->device, Ng);
+  if (!twg) return EZMOCK_ERR_UNKNOWN;
+  int R = 8;
+  while (R > 1 && sizeof(cplx) * (2 * (size_t) Nh + 1 + 2 * (size_t) Nh * R) > 160 * 1024) R >>= 1;
+  const size_t sm_r = sizeof(cplx) * (2 * (size_t) Nh + 1 + 2 * (size_t) Nh * R);
+  const int K = ez_fft_tile_k(Ng);
+  const size_t sm_a = sizeof(cplx) * ((size_t) Ng + 2 * (size_t) Ng * K);
+  static int attr_done = 0;
+  if (!attr_done) {
+    cudaFuncSetAttribute(fft_r2c_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(fft_axis_one<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done = 1;
+  }
+  const size_t nrows = (size_t) Ng * Ng;
+  fft_r2c_rows<<<(unsigned) ((nrows + R - 1) / R), FFT_NT, sm_r, m->stream>>>(
+      d_delta, m->spec[0], Ng, Nkp, R, nrows, ph, twg);
+  const int nkt = (m->Nk + K - 1) / K;
+  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, m->stream>>>(m->spec[0], Ng, Nkp, K, 1, pn);
+  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, m->stream>>>(m->spec[0], Ng, Nkp, K, 0, pn);
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+int ez_scale_psi(EzMesh *m, real f) {
+  scale_kernel<<<148 * 16, 256, 0, m->stream>>>(m->psi[0], 3 * m->N, f);
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}

@@ -1,0 +1,152 @@
+// ez_ic.cu -- Fourier-space initial field S(k) (the reference's `rhok`
+// before its multiplication by k_i; libEZmock/EZmock/perturb.c:78-359).
+//
+// Cell c of the half-complex grid (row-major, Ng x Ng x (Ng/2+1), origin
+// skipped) uses draws 2(c-1) (amplitude, get_double_pos) and 2(c-1)+1
+// (phase, get_double); with fixed amplitudes only draw c-1 (phase).  On the
+// k=0 and Nyquist planes the reference samples the lower half plane and
+// writes the partner (-i,-j) with its real part negated; here every thread
+// computes its own cell, upper-half cells from their partner's draws, so the
+// kernel needs no scattered writes.  The real parts at the seven non-origin
+// self-conjugate corners are zeroed (perturb.c:344-359).  All arithmetic is
+// FP64 (log, sqrt, sin, cos and the cubic-spline P(k)), rounded to `real` on
+// store, in the reference's expression order.
+#include "ez_internal.cuh"
+
+namespace {
+
+constexpr int IC_NT = 128;
+
+// bin search + natural cubic spline (linear_pk.c:36-51, 194-202;
+// cspline.c:91-105)
+__device__ __forceinline__ double pk_eval(const double *__restrict__ kt,
+    const double *__restrict__ Pt, const double *__restrict__ P2, int n,
+    double kv) {
+  int l = 0, u = n - 1, idx = -1;
+  while (l <= u) {
+    const int i = (l + u) >> 1;
+    if (i >= n - 1) { idx = (kt[n - 1] == kv) ? n - 1 : -1; break; }
+    if (kt[i + 1] <= kv) l = i + 1;
+    else if (kt[i] > kv) u = i - 1;
+    else { idx = i; break; }
+  }
+  if (idx == n - 1) return Pt[idx];
+  if (idx < 0) {
+    if (kv >= kt[n - 1]) return Pt[n - 1];
+    return Pt[0];
+  }
+  const int j = idx + 1;
+  const double ba = kt[j] - kt[idx];
+  const double xa = kv - kt[idx];
+  const double bx = kt[j] - kv;
+  const double ba2 = ba * ba;
+  const double lower = xa * Pt[j] + bx * Pt[idx];
+  const double c = (xa * xa - ba2) * xa * P2[j];
+  const double d = (bx * bx - ba2) * bx * P2[idx];
+  return (lower + 0x1.5555555555555p-3 * (c + d)) / ba;
+}
+
+__global__ void __launch_bounds__(IC_NT)
+ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
+    const double *__restrict__ tab, int npk, int logpk, int Ng, int Nk,
+    int Nkp, double kfac, double logkfac, double Pfac, int ran, int fixamp,
+    int iphase) {
+  const int Ngh = Ng >> 1;
+  const int row = blockIdx.x;                       // i * Ng + j
+  const int i = row / Ng, j = row - i * Ng;
+  const double ki = (i <= Ngh) ? i : i - Ng;
+  const double kj = (j <= Ngh) ? j : j - Ng;
+  const int ni = (i == 0) ? 0 : Ng - i, nj = (j == 0) ? 0 : Ng - j;
+  const double kij = ki * ki + kj * kj;
+  const bool lower = (i == ni && j <= Ngh) || (i != ni && i <= Ngh);
+  const bool selfp = (i == ni && j == nj);
+  const size_t rowc = (size_t) row * Nk;            // unpadded cell index base
+  const size_t prowc = ((size_t) ni * Ng + nj) * Nk;
+  const double *kt = tab, *Pt = tab + npk, *P2 = tab + 2 * npk;
+  const int per = fixamp ? 1 : 2;
+  for (int k = threadIdx.x; k < Nkp; k += blockDim.x) {
+    cplx out;
+    out.x = 0; out.y = 0;
+    const size_t c = rowc + k;
+    if (k < Nk && c != 0) {
+      const bool plane = (k == 0) || (((Ng & 1) == 0) && k == Ngh);
+      const size_t src = (!plane || lower) ? c : prowc + k;
+      const double ksq = kij + (double) (k * k);
+      const double kmod = logpk ? log(ksq) * 0.5 + logkfac : kfac * sqrt(ksq);
+      double P = pk_eval(kt, Pt, P2, npk, kmod);
+      double amp = 0;
+      if (!fixamp) amp = -log(ez_upos(ran, draws[(src - 1) * per]));
+      if (logpk) P = fixamp ? exp(P * 0.5) : exp(P * 0.5) * sqrt(amp);
+      else P = fixamp ? sqrt(P) : sqrt(P * amp);
+      P *= Pfac;
+      double phase = ez_u(ran, draws[(src - 1) * per + per - 1]) * 2 * EZ_PI;
+      if (iphase) phase += EZ_PI;
+      P /= (ksq * kfac);
+      real re = -P * sin(phase);
+      const real im = P * cos(phase);
+      if (plane && (!lower || selfp)) re = -re;
+      // self-conjugate corners: (0|Ngh, 0|Ngh, 0|Ngh) except the origin
+      if ((Ng & 1) == 0 && (i == 0 || i == Ngh) && (j == 0 || j == Ngh) &&
+          (k == 0 || k == Ngh))
+        re = 0;
+      out.x = re;
+      out.y = im;
+    }
+    S[(size_t) row * Nkp + k] = out;
+  }
+}
+
+// White-noise input: S = i sqrt(P)/(k^2 kf) L^-1.5 r2c(delta)
+// (perturb.c:476-554), applied to the forward transform already in S.
+__global__ void __launch_bounds__(IC_NT)
+wn_scale_kernel(cplx *__restrict__ S, const double *__restrict__ tab, int npk,
+    int logpk, int Ng, int Nk, int Nkp, double kfac, double logkfac,
+    double Pfac) {
+  const int Ngh = Ng >> 1;
+  const int row = blockIdx.x;
+  const int i = row / Ng, j = row - i * Ng;
+  const double ki = (i <= Ngh) ? i : i - Ng;
+  const double kj = (j <= Ngh) ? j : j - Ng;
+  const double kij = ki * ki + kj * kj;
+  const double *kt = tab, *Pt = tab + npk, *P2 = tab + 2 * npk;
+  for (int k = threadIdx.x; k < Nkp; k += blockDim.x) {
+    const size_t g = (size_t) row * Nkp + k;
+    cplx w = S[g], out;
+    out.x = 0; out.y = 0;
+    if (k < Nk && !(row == 0 && k == 0)) {
+      const double ksq = kij + (double) (k * k);
+      const double kmod = logpk ? log(ksq) * 0.5 + logkfac : kfac * sqrt(ksq);
+      double P = pk_eval(kt, Pt, P2, npk, kmod);
+      P = logpk ? exp(P * 0.5) : sqrt(P);
+      P *= Pfac / (ksq * kfac);
+      out.x = -P * w.y;
+      out.y = P * w.x;
+    }
+    S[g] = out;
+  }
+}
+
+}  // namespace
+
+int ez_ic_spectrum(EzMesh *m, const EzPk *pk, double Lbox, int ran,
+    int fixamp, int iphase, const uint32_t *draws) {
+  const int Ng = m->Ng;
+  const double kfac = EZ_PI * 2 / Lbox;
+  const double logkfac = log(kfac);
+  const double Pfac = pow(Lbox, -1.5);
+  ez_stage_begin(m, ST_IC);
+  ic_kernel<<<(unsigned) ((size_t) Ng * Ng), IC_NT, 0, m->stream>>>(
+      m->spec[0], draws, pk->d_tab, pk->n, pk->log ? 1 : 0, Ng, m->Nk, m->Nkp,
+      kfac, logkfac, Pfac, ran, fixamp, iphase);
+  ez_stage_end(m, ST_IC);
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+int ez_wn_scale(EzMesh *m, const EzPk *pk, double Lbox) {
+  const int Ng = m->Ng;
+  const double kfac = EZ_PI * 2 / Lbox;
+  wn_scale_kernel<<<(unsigned) ((size_t) Ng * Ng), IC_NT, 0, m->stream>>>(
+      m->spec[0], pk->d_tab, pk->n, pk->log ? 1 : 0, Ng, m->Nk, m->Nkp, kfac,
+      log(kfac), pow(Lbox, -1.5));
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}

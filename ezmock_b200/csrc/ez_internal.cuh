@@ -1,0 +1,147 @@
+// ez_internal.cuh -- shared declarations of the B200 EZmock engine.
+//
+// One library per precision: libEZmock_f32.so is built with -DSINGLE_PREC
+// (real = float), libEZmock_f64.so without (real = double), as the reference
+// selects `real` at compile time (libEZmock/EZmock/EZmock.h:38-42).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "EZmock.h"
+
+#ifdef SINGLE_PREC
+typedef float2 cplx;
+#define EZ_REAL_MIN 1.175494350822287508e-38f   // FLT_MIN
+#define EZ_REAL_TOL 1e-5                        // config.h:45-50
+#else
+typedef double2 cplx;
+#define EZ_REAL_MIN 2.2250738585072014e-308     // DBL_MIN
+#define EZ_REAL_TOL 1e-10
+#endif
+
+#define EZ_PI 0x1.921fb54442d18p+1
+#define EZ_NLOGB 64                 // config.h:64
+#define EZ_RHO_SAT 100              // config.h:71
+#define EZ_GAUSS_WIDTH 10           // config.h:73
+#define EZ_MAX_NT 1024              // config.h:59
+#define EZ_MAX_GRID 65536           // config.h:56
+#define EZ_MIN_TRACER 128           // config.h:58
+#define EZ_MAX_PK_N 1073741824      // config.h:57
+#define EZ_KMAX_BAO 0.5             // config.h:60
+#define EZ_DOUBLE_TOL 1e-8          // config.h:39
+
+// Spectral rows are padded to a multiple of this many complex values so that
+// every row starts on a 128-byte boundary and FFT column tiles are uniform.
+#define EZ_KPAD 16
+
+// ---- sub-structures of EZMOCK (layouts of the first members follow
+//      libEZmock/EZmock/structs.h:43-105 where callers may read them) ----
+struct EzConf {
+  int nthread;
+  int Ng;
+  double Lbox;
+};
+
+struct EzRng {
+  void *unused;            // the reference keeps its prand_t* here
+  int ran;                 // EZMOCK_RNG_MRG32K3A / EZMOCK_RNG_MT19937
+  uint64_t seed;
+};
+
+struct EzCosmo {
+  double growth2;
+  double vfac;
+};
+
+struct EzPk {
+  int n;
+  bool log;
+  double kmin, kmax;
+  double *k, *P, *P2;      // host copies
+  double *d_tab;           // device: k[n], P[n], P2[n]
+};
+
+struct EzPar {
+  double bao_enhance, rho_c, rho_exp, pdf_base, sigma_v;
+};
+
+// Per-stage device timings of the last calls (milliseconds).
+enum EzStage {
+  ST_RNG_IC = 0, ST_IC, ST_FFT_I, ST_FFT_J, ST_FFT_K, ST_CIC,
+  ST_BIAS, ST_SELECT, ST_EMIT, ST_VEL, ST_D2H, ST_NSTAGE
+};
+
+struct EzMesh {
+  bool rho_replaced, psi_ref, fixamp, iphase;
+  bool have_field;         // psi and rho on the device are valid
+  int device;
+  cudaStream_t stream;
+  cudaEvent_t ev[2 * ST_NSTAGE];
+  bool ev_used[ST_NSTAGE];
+  int timing;              // record per-stage events
+  int cic_mode;            // 0: float atomics, 1: deterministic fixed-point
+
+  int Ng;
+  size_t N;                // Ng^3
+  int Nk, Nkp;             // Ng/2+1 and its padded length
+  size_t Nspec;            // Ng*Ng*Nkp
+  real *psi[3];
+  real *rho;
+  real *paint[3];          // CIC of psi_d (un-normalised momenta)
+  cplx *spec[3];
+  uint32_t *draws;
+  size_t draws_cap;
+  void *scratch;           // general scratch (block sums, histograms, ...)
+  size_t scratch_cap;
+  void *rng_scratch;       // skip-ahead states of the MT19937 streams
+  size_t rng_scratch_cap;
+  unsigned long long *fixacc;   // deterministic CIC accumulators (4 x N)
+  real *cat;               // device catalogue (6 x cap)
+  size_t cat_cap;
+  real *h_stage;           // pinned host staging for the catalogue
+  size_t h_stage_cap;
+};
+
+// ---- error helpers ----
+#define EZ_CUDA_OK(call) (cudaSuccess == (call))
+
+// ---- RNG (ez_rng.cu) ----
+// Raw 32-bit draws [start, start+count) of the stream seeded by `seed`.
+int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
+    uint64_t count, uint32_t *out);
+// Conversions shared by all kernels (prand definitions of the oracle):
+//   MT19937  : u = x 2^-32 in [0,1); u_pos = (x + 0.5) 2^-32 in (0,1)
+//   MRG32k3a : u = u_pos = x * 2.328306549295727688e-10 in (0,1)
+__device__ __forceinline__ double ez_u(int ran, uint32_t x) {
+  return ran ? (double) x * (1.0 / 4294967296.0)
+             : (double) x * 2.328306549295727688e-10;
+}
+__device__ __forceinline__ double ez_upos(int ran, uint32_t x) {
+  return ran ? ((double) x + 0.5) * (1.0 / 4294967296.0)
+             : (double) x * 2.328306549295727688e-10;
+}
+
+// ---- stages ----
+int ez_ic_spectrum(EzMesh *m, const EzPk *pk, double Lbox, int ran,
+    int fixamp, int iphase, const uint32_t *draws);
+int ez_whitenoise_spectrum(EzMesh *m, const EzPk *pk, double Lbox,
+    const real *d_delta);
+int ez_fft_c2r_psi(EzMesh *m);
+int ez_cic(EzMesh *m, double Lbox);
+
+struct EzPopResult {
+  size_t ntot, ncell, nvalid;
+  int err;
+};
+int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
+    double vfac, const real *params, const size_t *pdf, int nmax,
+    size_t ncell, size_t ntot, EzPopResult *res);
+
+// ---- memory ----
+int ez_mesh_alloc(EzMesh *m, int Ng);
+int ez_scratch(EzMesh *m, size_t bytes);
+int ez_rng_scratch(EzMesh *m, size_t bytes);
+void ez_stage_begin(EzMesh *m, int st);
+void ez_stage_end(EzMesh *m, int st);

@@ -1,0 +1,601 @@
+// ez_pop.cu -- tracer population on the GPU
+// (libEZmock/EZmock/pop_tracer.c:149-1113, serial semantics).
+//
+//  1. valid cells (rho >= rho_c) counted per 4096-cell chunk, scanned, so each
+//     valid cell knows its rank r in index order;
+//  2. bias: pair p = r/2 takes draws 2N+2p (radius) and 2N+2p+1 (angle);
+//     even r uses cos, odd r sin (gauss_rand, :70-79); rho_t = (1 -
+//     exp(-min(rho,100)/rho_exp)) G with G = 1+g or exp(g); log2 histogram
+//     of rho_t (:170-172, :264-270);
+//  3. selection (:359-509): cells with rho_t above the histogram cut are
+//     compacted, their keys sorted (LSD radix sort), and PDF bin j takes the
+//     next pdf[j] cells in descending order plus every further cell equal to
+//     the smallest one taken (tie extension, :436-446).  Bin j is then the
+//     value interval [lo_j, lo_{j-1}), so per-cell counts follow from rho_t
+//     alone;
+//  4. emission (:894-994): tracer t (cell-index order) takes draws
+//     5N+3t..5N+3t+2 for its position in the cell;
+//  5. velocities (:593-753): mass-weighted CIC gather of the momentum grids
+//     painted during the density assignment, times vfac;
+//  6. dispersion (:1043-1113): tracer pair m takes draws 8N+6m..8N+6m+5 as
+//     three Box-Muller pairs.
+#include "ez_internal.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace {
+
+constexpr int NT = 256;
+constexpr int ROWS = 16;
+constexpr int CH = NT * ROWS;           // cells per chunk
+
+#ifdef SINGLE_PREC
+typedef uint32_t skey_t;
+__device__ __forceinline__ skey_t to_key(real v) { return ~__float_as_uint(v); }
+__device__ __forceinline__ real from_key(skey_t k) { return __uint_as_float(~k); }
+#else
+typedef unsigned long long skey_t;
+__device__ __forceinline__ skey_t to_key(real v) { return ~(skey_t) __double_as_longlong(v); }
+__device__ __forceinline__ real from_key(skey_t k) { return __longlong_as_double((long long) ~k); }
+#endif
+
+// exclusive block scan over NT threads; returns the prefix, writes the total
+template <typename T>
+__device__ __forceinline__ T block_scan(T v, T *total, T *sw) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sw[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    T s = (lane < (int) (blockDim.x >> 5)) ? sw[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    sw[lane] = s;                       // inclusive warp-total prefix
+  }
+  __syncthreads();
+  const T before = (w ? sw[w - 1] : 0) + x - v;
+  *total = sw[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before;
+}
+
+__device__ __forceinline__ int logb_bin(real v) {
+  // 5 - ilogb(v) clamped to [0,63]; exactly zero goes to the last bin
+  if (v == 0) return EZ_NLOGB - 1;
+  int idx = 5 - ilogb((double) v);
+  return idx < 0 ? 0 : (idx >= EZ_NLOGB ? EZ_NLOGB - 1 : idx);
+}
+
+__global__ void __launch_bounds__(NT)
+valid_count_kernel(const real *__restrict__ rho, size_t N, real thres,
+    unsigned long long *cnt) {
+  __shared__ unsigned long long sw[32];
+  unsigned long long c = 0;
+  const size_t b0 = (size_t) blockIdx.x * CH;
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    if (id < N && !(rho[id] < thres)) c++;
+  }
+  unsigned long long tot;
+  block_scan<unsigned long long>(c, &tot, sw);
+  if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
+}
+
+// single-block exclusive scan of n values; out[n] = total
+__global__ void __launch_bounds__(1024)
+scan_kernel(const unsigned long long *__restrict__ in, unsigned long long *out,
+    size_t n) {
+  __shared__ unsigned long long sw[32];
+  const size_t per = (n + blockDim.x - 1) / blockDim.x;
+  const size_t s0 = threadIdx.x * per, s1 = min(n, s0 + per);
+  unsigned long long loc = 0;
+  for (size_t i = s0; i < s1; i++) loc += in[i];
+  unsigned long long tot;
+  unsigned long long run = block_scan<unsigned long long>(loc, &tot, sw);
+  for (size_t i = s0; i < s1; i++) { const unsigned long long v = in[i]; out[i] = run; run += v; }
+  if (threadIdx.x == 0) out[n] = tot;
+}
+
+__global__ void __launch_bounds__(NT)
+bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
+    real thres, double iexp, double lambda, const unsigned long long *off,
+    const uint32_t *__restrict__ draws, int ran, unsigned long long *hist) {
+  __shared__ unsigned long long sw[32];
+  __shared__ unsigned int sh[EZ_NLOGB];
+  if (threadIdx.x < EZ_NLOGB) sh[threadIdx.x] = 0;
+  __syncthreads();
+  unsigned long long run = off[blockIdx.x];
+  const size_t b0 = (size_t) blockIdx.x * CH;
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    real r = 0;
+    bool valid = false;
+    if (id < N) { r = rho[id]; valid = !(r < thres); }
+    unsigned long long tot;
+    const unsigned long long rank = run + block_scan<unsigned long long>(valid ? 1ULL : 0ULL, &tot, sw);
+    run += tot;
+    if (id >= N) continue;
+    if (!valid) { rhot[id] = 0; continue; }
+    const real v = (r > (real) EZ_RHO_SAT) ? (real) EZ_RHO_SAT : r;
+    const unsigned long long p = rank >> 1;
+    const double rr = -2 * log(ez_upos(ran, draws[2 * p]));
+    const double th = ez_u(ran, draws[2 * p + 1]) * 2 * EZ_PI;
+    double g = (rank & 1) ? lambda * sqrt(rr) * sin(th) : lambda * sqrt(rr) * cos(th);
+    g = (g >= 0) ? 1 + g : exp(g);
+    const real t = (1 - exp((double) v * iexp)) * g;
+    rhot[id] = t;
+    atomicAdd(&sh[logb_bin(t)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < EZ_NLOGB && sh[threadIdx.x])
+    atomicAdd(hist + threadIdx.x, (unsigned long long) sh[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(NT)
+compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
+    skey_t *__restrict__ keys, unsigned long long *counter) {
+  for (size_t id = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+       id - threadIdx.x < N; id += (size_t) gridDim.x * blockDim.x) {
+    bool take = false;
+    real v = 0;
+    if (id < N) { v = rhot[id]; take = !(v < thres); }
+    const unsigned mask = __ballot_sync(0xffffffffu, take);
+    if (!mask) continue;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(counter, (unsigned long long) __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (take) keys[base + __popc(mask & ((1u << lane) - 1))] = to_key(v);
+  }
+}
+
+// ---- LSD radix sort of keys (ascending), 8-bit digits ----
+constexpr int SORT_NT = 256;
+constexpr int SORT_PER = 8;
+constexpr int TILE = SORT_NT * SORT_PER;
+
+__global__ void __launch_bounds__(SORT_NT)
+digit_hist_kernel(const skey_t *__restrict__ keys, size_t M, int shift,
+    unsigned long long *counts, size_t ntiles) {
+  __shared__ unsigned int h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const size_t t0 = (size_t) blockIdx.x * TILE;
+  for (int e = threadIdx.x; e < TILE; e += SORT_NT) {
+    const size_t g = t0 + e;
+    if (g < M) atomicAdd(&h[(keys[g] >> shift) & 255], 1u);
+  }
+  __syncthreads();
+  counts[(size_t) threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(SORT_NT)
+digit_scatter_kernel(const skey_t *__restrict__ in, skey_t *__restrict__ out,
+    size_t M, int shift, const unsigned long long *__restrict__ offs,
+    size_t ntiles) {
+  __shared__ skey_t sk[TILE];
+  __shared__ unsigned int sw[32];
+  __shared__ unsigned int dstart[256];
+  const size_t t0 = (size_t) blockIdx.x * TILE;
+  const int n = (int) min((size_t) TILE, M - t0);
+  // thread t holds keys at tile positions t*PER .. t*PER+PER-1
+  skey_t k[SORT_PER];
+#pragma unroll
+  for (int j = 0; j < SORT_PER; j++) {
+    const int pos = threadIdx.x * SORT_PER + j;
+    k[j] = (pos < n) ? in[t0 + pos] : ~(skey_t) 0;
+  }
+  // stable sort of the tile by the 8-bit digit: eight 1-bit splits
+  for (int b = 0; b < 8; b++) {
+    unsigned int zeros = 0;
+#pragma unroll
+    for (int j = 0; j < SORT_PER; j++) zeros += !((k[j] >> (shift + b)) & 1);
+    unsigned int tz;
+    unsigned int zb = block_scan<unsigned int>(zeros, &tz, sw);
+    unsigned int ob = threadIdx.x * SORT_PER - zb;
+#pragma unroll
+    for (int j = 0; j < SORT_PER; j++) {
+      const bool one = (k[j] >> (shift + b)) & 1;
+      const unsigned int dst = one ? tz + ob++ : zb++;
+      sk[dst] = k[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < SORT_PER; j++) k[j] = sk[threadIdx.x * SORT_PER + j];
+    __syncthreads();
+  }
+  // local start of each digit (padding keys have digit 255 and sort last)
+  dstart[threadIdx.x] = 0xffffffffu;
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < SORT_PER; j++) {
+    const int pos = threadIdx.x * SORT_PER + j;
+    const int d = (int) ((k[j] >> shift) & 255);
+    const int dprev = pos ? (int) ((sk[pos - 1] >> shift) & 255) : -1;
+    if (pos < n && d != dprev) dstart[d] = pos;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < SORT_PER; j++) {
+    const int pos = threadIdx.x * SORT_PER + j;
+    if (pos >= n) continue;
+    const int d = (int) ((k[j] >> shift) & 255);
+    out[offs[(size_t) d * ntiles + blockIdx.x] + (pos - dstart[d])] = k[j];
+  }
+}
+
+// ---- boundaries of the PDF bins (one thread; pop_tracer.c:405-461) ----
+struct BoundOut {
+  unsigned long long ncell, ntot;
+  int err;
+  int nbins;                 // number of non-empty bins
+  real lo[EZ_MAX_NT];        // lowest rho_t of each non-empty bin
+  int ntr[EZ_MAX_NT];        // tracers per cell of that bin
+  unsigned long long pdf[EZ_MAX_NT];
+};
+
+__device__ size_t upper_bound_key(const skey_t *a, size_t lo, size_t hi, skey_t v) {
+  while (lo < hi) {
+    const size_t mid = (lo + hi) >> 1;
+    if (a[mid] <= v) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void bounds_kernel(const skey_t *__restrict__ keys, size_t M,
+    const unsigned long long *__restrict__ pdf, int nmax,
+    unsigned long long ncell, unsigned long long ntot, BoundOut *o) {
+  size_t P = 0;
+  int nb = 0;
+  o->err = 0;
+  for (int j = 0; j < nmax; j++) {
+    unsigned long long q = pdf[j];
+    if (!q) { o->pdf[j] = 0; continue; }
+    size_t E = P + q;
+    if (E > M) { o->err = EZMOCK_ERR_UNKNOWN; return; }
+    const size_t E2 = upper_bound_key(keys, E, M, keys[E - 1]);
+    const unsigned long long extra = E2 - E;
+    q += extra;
+    ncell += extra;
+    ntot += extra * (unsigned long long) (nmax - j);
+    E = E2;
+    o->pdf[j] = q;
+    o->lo[nb] = from_key(keys[E - 1]);
+    o->ntr[nb] = nmax - j;
+    nb++;
+    P = E;
+  }
+  o->nbins = nb;
+  o->ncell = ncell;
+  o->ntot = ntot;
+}
+
+__device__ __forceinline__ int cell_count(real v, const real *lo, const int *ntr,
+    int nb) {
+  // first non-empty bin (descending thresholds) with v >= lo
+  if (!nb || v < lo[nb - 1] || !(v == v)) return 0;
+  int a = 0, b = nb - 1;
+  while (a < b) {
+    const int mid = (a + b) >> 1;
+    if (v >= lo[mid]) b = mid; else a = mid + 1;
+  }
+  return ntr[a];
+}
+
+__global__ void __launch_bounds__(NT)
+tracer_count_kernel(const real *__restrict__ rhot, size_t N,
+    const BoundOut *__restrict__ bo, unsigned long long *cnt) {
+  __shared__ real slo[EZ_MAX_NT];
+  __shared__ int sntr[EZ_MAX_NT];
+  __shared__ unsigned long long sw[32];
+  const int nb = bo->nbins;
+  for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
+  __syncthreads();
+  unsigned long long c = 0;
+  const size_t b0 = (size_t) blockIdx.x * CH;
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    if (id < N) c += cell_count(rhot[id], slo, sntr, nb);
+  }
+  unsigned long long tot;
+  block_scan<unsigned long long>(c, &tot, sw);
+  if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(NT)
+emit_kernel(const real *__restrict__ rhot, size_t N, int Ng,
+    const BoundOut *__restrict__ bo, const unsigned long long *__restrict__ off,
+    const uint32_t *__restrict__ draws, int ran, real gs, double Lbox,
+    unsigned long long ntr, real *x, real *y, real *z) {
+  __shared__ real slo[EZ_MAX_NT];
+  __shared__ int sntr[EZ_MAX_NT];
+  __shared__ unsigned long long sw[32];
+  const int nb = bo->nbins;
+  for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
+  __syncthreads();
+  unsigned long long run = off[blockIdx.x];
+  const size_t b0 = (size_t) blockIdx.x * CH;
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    const int n = (id < N) ? cell_count(rhot[id], slo, sntr, nb) : 0;
+    unsigned long long tot;
+    const unsigned long long t0 = run + block_scan<unsigned long long>((unsigned long long) n, &tot, sw);
+    run += tot;
+    if (!n) continue;
+    const int kk = (int) (id % Ng);
+    const size_t ij = id / Ng;
+    const int jj = (int) (ij % Ng), ii = (int) (ij / Ng);
+    for (int m = 0; m < n; m++) {
+      const unsigned long long t = t0 + m;
+      if (t >= ntr) break;
+      double r = ez_u(ran, draws[3 * t]) - 0.5;
+      real xx = (ii + r) * (double) gs;
+      r = ez_u(ran, draws[3 * t + 1]) - 0.5;
+      real yy = (jj + r) * (double) gs;
+      r = ez_u(ran, draws[3 * t + 2]) - 0.5;
+      real zz = (kk + r) * (double) gs;
+      if (xx < 0) xx = (double) xx + Lbox;
+      if (yy < 0) yy = (double) yy + Lbox;
+      if (zz < 0) zz = (double) zz + Lbox;
+      x[t] = xx; y[t] = yy; z[t] = zz;
+    }
+  }
+}
+
+__device__ __forceinline__ size_t idx3(int Ng, int a, int b, int c) {
+  return ((size_t) a * Ng + b) * Ng + c;
+}
+
+__device__ __forceinline__ real norm_paint(const real *q, const real *rho,
+    size_t c) {
+  const real r = rho[c];
+  return (r > (real) EZ_REAL_TOL) ? q[c] / r : q[c];
+}
+
+__global__ void __launch_bounds__(NT)
+vel_kernel(const real *__restrict__ rho, const real *__restrict__ q0,
+    const real *__restrict__ q1, const real *__restrict__ q2, int Ng, real igs,
+    double vfac, size_t n, const real *__restrict__ x, const real *__restrict__ y,
+    const real *__restrict__ z, real *vx, real *vy, real *vz) {
+  for (size_t t = (size_t) blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (size_t) gridDim.x * blockDim.x) {
+    const real xx = x[t] * igs, yy = y[t] * igs, zz = z[t] * igs;
+    int x0 = (int) xx, y0 = (int) yy, z0 = (int) zz;
+    const real wx1 = xx - x0, wx0 = 1 - wx1;
+    const real wy1 = yy - y0, wy0 = 1 - wy1;
+    const real wz1 = zz - z0, wz0 = 1 - wz1;
+    if (x0 == Ng) x0 = 0;
+    if (y0 == Ng) y0 = 0;
+    if (z0 == Ng) z0 = 0;
+    const int x1 = (x0 == Ng - 1) ? 0 : x0 + 1;
+    const int y1 = (y0 == Ng - 1) ? 0 : y0 + 1;
+    const int z1 = (z0 == Ng - 1) ? 0 : z0 + 1;
+    const size_t cs[8] = {idx3(Ng, x0, y0, z0), idx3(Ng, x0, y0, z1),
+                          idx3(Ng, x0, y1, z0), idx3(Ng, x0, y1, z1),
+                          idx3(Ng, x1, y0, z0), idx3(Ng, x1, y0, z1),
+                          idx3(Ng, x1, y1, z0), idx3(Ng, x1, y1, z1)};
+    const real wa[8] = {wx0, wx0, wx0, wx0, wx1, wx1, wx1, wx1};
+    const real wb[8] = {wy0, wy0, wy1, wy1, wy0, wy0, wy1, wy1};
+    const real wc[8] = {wz0, wz1, wz0, wz1, wz0, wz1, wz0, wz1};
+    real rw[8];
+    real rs = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      rw[c] = rho[cs[c]] * wa[c] * wb[c] * wc[c];
+      rs = (c == 0) ? rw[0] : rs + rw[c];
+    }
+    const double fac = vfac / rs;
+    real *outs[3] = {vx, vy, vz};
+    const real *qs[3] = {q0, q1, q2};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      real v = 0;
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const real pr = norm_paint(qs[d], rho, cs[c]) * rw[c];
+        v = (c == 0) ? pr : v + pr;
+      }
+      outs[d][t] = v * fac;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+disp_kernel(size_t n, const uint32_t *__restrict__ draws, int ran,
+    double sigma, real *vx, real *vy, real *vz) {
+  const size_t npair = (n + 1) / 2;
+  for (size_t m = (size_t) blockIdx.x * blockDim.x + threadIdx.x; m < npair;
+       m += (size_t) gridDim.x * blockDim.x) {
+    double g[6];
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+      const double rr = -2 * log(ez_upos(ran, draws[6 * m + 2 * p]));
+      const double th = ez_u(ran, draws[6 * m + 2 * p + 1]) * 2 * EZ_PI;
+      g[2 * p] = sigma * sqrt(rr) * cos(th);
+      g[2 * p + 1] = sigma * sqrt(rr) * sin(th);
+    }
+    const size_t a = 2 * m;
+    vx[a] = vx[a] + g[0];
+    vy[a] = vy[a] + g[1];
+    vz[a] = vz[a] + g[2];
+    if (a + 1 < n) {
+      vx[a + 1] = vx[a + 1] + g[3];
+      vy[a + 1] = vy[a + 1] + g[4];
+      vz[a + 1] = vz[a + 1] + g[5];
+    }
+  }
+}
+
+unsigned grid_for(size_t n, int nt) {
+  const size_t b = (n + nt - 1) / nt;
+  return (unsigned) (b < 148 * 32 ? (b ? b : 1) : 148 * 32);
+}
+
+int ensure_draws(EzMesh *m, size_t count) {
+  if (count <= m->draws_cap) return 0;
+  if (m->draws) cudaFree(m->draws);
+  m->draws = nullptr;
+  if (!EZ_CUDA_OK(cudaMalloc(&m->draws, count * sizeof(uint32_t)))) {
+    m->draws_cap = 0;
+    return EZMOCK_ERR_MEMORY;
+  }
+  m->draws_cap = count;
+  return 0;
+}
+
+}  // namespace
+
+int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
+    double vfac, const real *params, const size_t *pdf, int nmax,
+    size_t ncell, size_t ntot, EzPopResult *res) {
+  const size_t N = m->N;
+  const real rho_c = params[0], rho_exp = params[1], sigma_v = params[3];
+  const real thres = (rho_c == 0) ? (real) EZ_REAL_MIN : rho_c;
+  const double iexp = -1 / rho_exp;
+  const size_t nblk = (N + CH - 1) / CH;
+  int e;
+  res->err = 0;
+
+  // scratch: block counts (nblk+1) x2, hist 64, bounds struct, pdf copy,
+  // sort digit counts (256 x tiles + 1)
+  const size_t ntile_max = (N + TILE - 1) / TILE;
+  const size_t off_cnt = 0;
+  const size_t off_scan = off_cnt + (nblk + 1) * 8;
+  const size_t off_hist = off_scan + (nblk + 1) * 8;
+  const size_t off_bo = (off_hist + EZ_NLOGB * 8 + 255) / 256 * 256;
+  const size_t off_pdf = (off_bo + sizeof(BoundOut) + 255) / 256 * 256;
+  const size_t off_dc = (off_pdf + EZ_MAX_NT * 8 + 255) / 256 * 256;
+  const size_t off_dcs = off_dc + (256 * ntile_max + 1) * 8;
+  const size_t off_ctr = off_dcs + (256 * ntile_max + 1) * 8;
+  if ((e = ez_scratch(m, off_ctr + 64))) return e;
+  char *sc = (char *) m->scratch;
+  unsigned long long *bcnt = (unsigned long long *) (sc + off_cnt);
+  unsigned long long *bscan = (unsigned long long *) (sc + off_scan);
+  unsigned long long *hist = (unsigned long long *) (sc + off_hist);
+  BoundOut *bo = (BoundOut *) (sc + off_bo);
+  unsigned long long *dpdf = (unsigned long long *) (sc + off_pdf);
+  unsigned long long *dcount = (unsigned long long *) (sc + off_dc);
+  unsigned long long *dcscan = (unsigned long long *) (sc + off_dcs);
+  unsigned long long *counter = (unsigned long long *) (sc + off_ctr);
+
+  real *rhot = (real *) m->spec[0];
+  skey_t *keys_a = (skey_t *) m->spec[1];
+  skey_t *keys_b = (skey_t *) m->spec[2];
+  cudaStream_t st = m->stream;
+
+  // ---- 1. valid ranks ----
+  ez_stage_begin(m, ST_BIAS);
+  valid_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, N, thres, bcnt);
+  scan_kernel<<<1, 1024, 0, st>>>(bcnt, bscan, nblk);
+  unsigned long long nvalid = 0;
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(&nvalid, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+    return EZMOCK_ERR_UNKNOWN;
+  res->nvalid = nvalid;
+  if (nvalid < ncell) { res->err = EZMOCK_ERR_RHO_LESS; return 0; }
+
+  // ---- 2. bias ----
+  const size_t nd_bias = nvalid + (nvalid & 1);
+  if ((e = ensure_draws(m, std::max(nd_bias, (size_t) 1)))) return e;
+  if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N << 1, nd_bias, m->draws))) return e;
+  cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
+  bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
+      (double) (real) EZ_GAUSS_WIDTH, bscan, m->draws, ran, hist);
+  unsigned long long h[EZ_NLOGB];
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+    return EZMOCK_ERR_UNKNOWN;
+  ez_stage_end(m, ST_BIAS);
+
+  // ---- 3. selection ----
+  ez_stage_begin(m, ST_SELECT);
+  int imax;
+  size_t cnt = 0;
+  for (imax = 0; imax < EZ_NLOGB; imax++) {
+    cnt += h[imax];
+    if (cnt >= ncell) break;
+  }
+  const real ilogb_max = 5;
+  const real cut = (imax == EZ_NLOGB - 1) ? (real) EZ_REAL_MIN
+      : (real) pow(2.0, (double) ilogb_max - imax);
+  cudaMemsetAsync(counter, 0, 8, st);
+  compact_kernel<<<grid_for(N, NT), NT, 0, st>>>(rhot, N, cut, keys_a, counter);
+  unsigned long long M = 0;
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(&M, counter, 8, cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+    return EZMOCK_ERR_UNKNOWN;
+  skey_t *sorted = keys_a;
+  if (M > 1) {
+    const size_t ntiles = (M + TILE - 1) / TILE;
+    skey_t *src = keys_a, *dst = keys_b;
+    for (int shift = 0; shift < (int) (8 * sizeof(skey_t)); shift += 8) {
+      digit_hist_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, M, shift, dcount, ntiles);
+      scan_kernel<<<1, 1024, 0, st>>>(dcount, dcscan, 256 * ntiles);
+      digit_scatter_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, dst, M, shift, dcscan, ntiles);
+      skey_t *t = src; src = dst; dst = t;
+    }
+    sorted = src;
+  }
+  std::vector<unsigned long long> hp(nmax);
+  for (int j = 0; j < nmax; j++) hp[j] = pdf[j];
+  cudaMemcpyAsync(dpdf, hp.data(), nmax * 8, cudaMemcpyHostToDevice, st);
+  bounds_kernel<<<1, 1, 0, st>>>(sorted, M, dpdf, nmax, ncell, ntot, bo);
+  struct { unsigned long long ncell, ntot; int err; int nbins; } hb;
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(&hb, bo, sizeof(hb), cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+    return EZMOCK_ERR_UNKNOWN;
+  ez_stage_end(m, ST_SELECT);
+  if (hb.err) { res->err = hb.err; return 0; }
+  res->ncell = hb.ncell;
+  res->ntot = hb.ntot;
+  const size_t nt_all = hb.ntot;
+
+  // ---- 4. emission ----
+  ez_stage_begin(m, ST_EMIT);
+  if (nt_all > m->cat_cap) {
+    if (m->cat) cudaFree(m->cat);
+    m->cat = nullptr;
+    m->cat_cap = 0;
+    if (!EZ_CUDA_OK(cudaMalloc(&m->cat, 6 * nt_all * sizeof(real)))) return EZMOCK_ERR_MEMORY;
+    m->cat_cap = nt_all;
+  }
+  real *cx = m->cat, *cy = cx + nt_all, *cz = cy + nt_all;
+  real *cvx = cz + nt_all, *cvy = cvx + nt_all, *cvz = cvy + nt_all;
+  tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt);
+  scan_kernel<<<1, 1024, 0, st>>>(bcnt, bscan, nblk);
+  unsigned long long ncount = 0;
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(&ncount, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+    return EZMOCK_ERR_UNKNOWN;
+  // the per-cell counts must add up to the selected total (pop_tracer.c:989-993)
+  if (ncount != nt_all) { res->err = EZMOCK_ERR_UNKNOWN; return 0; }
+  if ((e = ensure_draws(m, std::max((size_t) 3 * nt_all, (size_t) 1)))) return e;
+  if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N * 5, 3 * nt_all, m->draws))) return e;
+  const real gs = Lbox / Ng;
+  emit_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, Ng, bo, bscan, m->draws,
+      ran, gs, Lbox, (unsigned long long) nt_all, cx, cy, cz);
+  ez_stage_end(m, ST_EMIT);
+
+  // ---- 5./6. velocities and dispersion ----
+  ez_stage_begin(m, ST_VEL);
+  const real igs = Ng / Lbox;
+  vel_kernel<<<grid_for(nt_all, NT), NT, 0, st>>>(m->rho, m->paint[0],
+      m->paint[1], m->paint[2], Ng, igs, vfac, nt_all, cx, cy, cz, cvx, cvy, cvz);
+  const size_t nd_disp = 6 * ((nt_all + 1) / 2);
+  if ((e = ensure_draws(m, std::max(nd_disp, (size_t) 1)))) return e;
+  if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N << 3, nd_disp, m->draws))) return e;
+  disp_kernel<<<grid_for((nt_all + 1) / 2, NT), NT, 0, st>>>(nt_all, m->draws,
+      ran, (double) sigma_v, cvx, cvy, cvz);
+  ez_stage_end(m, ST_VEL);
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}

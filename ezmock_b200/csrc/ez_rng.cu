@@ -1,0 +1,509 @@
+// ez_rng.cu -- GPU random streams with absolute skip-ahead.
+//
+// EZmock addresses every random draw by an absolute index of one stream per
+// seed: `reset(state, seed, s)` then sequential draws
+// (libEZmock/EZmock/perturb.c:112-118, pop_tracer.c:233-237, :919, :1071).
+// The generator library (`prand`) is not part of the reference tree; the
+// definitions here are the published algorithms, with the seeding and draw
+// conversions documented in ez_internal.cuh:
+//
+//  * MRG32k3a (L'Ecuyer 1999): every block jumps to its first draw with
+//    precomputed powers A^(2^k) of the 3x3 transition matrices, every thread
+//    then jumps to its sub-chunk with A^(t*G) and generates G draws, which
+//    are transposed through shared memory so global stores are coalesced.
+//
+//  * MT19937 (Matsumoto & Nishimura 1998): the 624-word window of the stream
+//    at any offset J is p(T) applied to the seed window, p = x^J mod phi
+//    (Haramoto et al. 2008).  phi is found once on the host by
+//    Berlekamp-Massey and the table x^(2^k) mod phi by repeated squaring.  On
+//    the GPU one block applies p(T) with Horner's rule over 6-bit windows
+//    (a 64-entry table of combinations of T^j s held in shared memory, one
+//    barrier per window).  Chunk states for a range [start, start + P*L) are
+//    built by one jump to `start` followed by log2(P) doubling levels, each
+//    level jumping all known chunk states by 2^m * L in parallel.  Each chunk
+//    is then generated by one block with the three-phase twist.
+#include "ez_internal.cuh"
+
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+namespace {
+
+// ============================================================================
+//                                 MRG32k3a
+// ============================================================================
+
+constexpr uint64_t M1 = 4294967087ULL, M2 = 4294944443ULL;
+constexpr uint32_t C1 = 209, C2 = 22853;          // m = 2^32 - c
+constexpr uint64_t A12 = 1403580, A13N = 810728, A21 = 527612, A23N = 1370589;
+
+constexpr int MRG_THREADS = 128;
+constexpr int MRG_G = 64;                          // draws per thread
+constexpr int MRG_BLOCK = MRG_THREADS * MRG_G;     // draws per block
+
+__constant__ uint32_t c_mrg_pow1[64][9];
+__constant__ uint32_t c_mrg_pow2[64][9];
+
+__device__ __forceinline__ uint32_t mod_special(uint64_t x, uint32_t c) {
+  const uint64_t m = (1ULL << 32) - c;
+  uint64_t y = (x >> 32) * c + (x & 0xffffffffULL);
+  y = (y >> 32) * c + (y & 0xffffffffULL);
+  if (y >= m) y -= m;
+  if (y >= m) y -= m;
+  return (uint32_t) y;
+}
+
+__device__ __forceinline__ void matvec(const uint32_t *a, uint32_t *v,
+    uint32_t c) {
+  const uint64_t m = (1ULL << 32) - c;
+  uint32_t t[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    uint64_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      s += mod_special((uint64_t) a[3 * i + k] * v[k], c);
+    while (s >= m) s -= m;
+    t[i] = (uint32_t) s;
+  }
+  v[0] = t[0]; v[1] = t[1]; v[2] = t[2];
+}
+
+__device__ __forceinline__ uint32_t mrg_step(uint32_t *s1, uint32_t *s2) {
+  uint64_t p1 = (uint64_t) mod_special(A12 * s1[1], C1) +
+                mod_special((M1 - A13N) * s1[0], C1);
+  if (p1 >= M1) p1 -= M1;
+  uint64_t p2 = (uint64_t) mod_special(A21 * s2[2], C2) +
+                mod_special((M2 - A23N) * s2[0], C2);
+  if (p2 >= M2) p2 -= M2;
+  s1[0] = s1[1]; s1[1] = s1[2]; s1[2] = (uint32_t) p1;
+  s2[0] = s2[1]; s2[1] = s2[2]; s2[2] = (uint32_t) p2;
+  return (uint32_t) ((p1 > p2) ? p1 - p2 : p1 + M1 - p2);
+}
+
+__global__ void __launch_bounds__(MRG_THREADS)
+mrg_fill_kernel(uint32_t s10, uint32_t s11, uint32_t s12, uint32_t s20,
+    uint32_t s21, uint32_t s22, uint64_t start, uint64_t count,
+    const uint32_t *__restrict__ thread_jump, uint32_t *__restrict__ out) {
+  __shared__ uint32_t sbuf[MRG_THREADS * (MRG_G + 1)];
+  __shared__ uint32_t bstate[6];
+  const uint64_t b0 = (uint64_t) blockIdx.x * MRG_BLOCK;
+  if (threadIdx.x == 0) {
+    uint32_t v1[3] = {s10, s11, s12}, v2[3] = {s20, s21, s22};
+    uint64_t J = start + b0;
+    for (int k = 0; J; k++, J >>= 1) {
+      if (J & 1) {
+        matvec(c_mrg_pow1[k], v1, C1);
+        matvec(c_mrg_pow2[k], v2, C2);
+      }
+    }
+    for (int i = 0; i < 3; i++) { bstate[i] = v1[i]; bstate[3 + i] = v2[i]; }
+  }
+  __syncthreads();
+  uint32_t v1[3] = {bstate[0], bstate[1], bstate[2]};
+  uint32_t v2[3] = {bstate[3], bstate[4], bstate[5]};
+  const int t = threadIdx.x;
+  if (t) {
+    matvec(thread_jump + 18 * t, v1, C1);
+    matvec(thread_jump + 18 * t + 9, v2, C2);
+  }
+#pragma unroll 4
+  for (int i = 0; i < MRG_G; i++) sbuf[t * (MRG_G + 1) + i] = mrg_step(v1, v2);
+  __syncthreads();
+  for (int e = t; e < MRG_BLOCK; e += MRG_THREADS) {
+    const uint64_t g = b0 + e;
+    if (g < count) out[g] = sbuf[(e / MRG_G) * (MRG_G + 1) + (e % MRG_G)];
+  }
+}
+
+// host-side 3x3 arithmetic modulo m
+void hmat_mul(const uint64_t *a, const uint64_t *b, uint64_t *c, uint64_t m) {
+  uint64_t t[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      unsigned __int128 s = 0;
+      for (int k = 0; k < 3; k++) s += (unsigned __int128) a[3 * i + k] * b[3 * k + j];
+      t[3 * i + j] = (uint64_t) (s % m);
+    }
+  memcpy(c, t, sizeof(t));
+}
+
+uint64_t splitmix64(uint64_t *z) {
+  uint64_t r = (*z += 0x9e3779b97f4a7c15ULL);
+  r = (r ^ (r >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  r = (r ^ (r >> 27)) * 0x94d049bb133111ebULL;
+  return r ^ (r >> 31);
+}
+
+std::mutex g_mrg_mu;
+int g_mrg_dev_ready = -1;                 // device id whose tables are set
+uint32_t *g_mrg_thread_jump = nullptr;    // device, MRG_THREADS x 18
+
+int mrg_prepare(int dev) {
+  std::lock_guard<std::mutex> lk(g_mrg_mu);
+  if (g_mrg_dev_ready == dev) return 0;
+  uint64_t p1[64][9], p2[64][9];
+  const uint64_t a1[9] = {0, 1, 0, 0, 0, 1, M1 - A13N, A12, 0};
+  const uint64_t a2[9] = {0, 1, 0, 0, 0, 1, M2 - A23N, 0, A21};
+  memcpy(p1[0], a1, sizeof(a1));
+  memcpy(p2[0], a2, sizeof(a2));
+  for (int k = 1; k < 64; k++) {
+    hmat_mul(p1[k - 1], p1[k - 1], p1[k], M1);
+    hmat_mul(p2[k - 1], p2[k - 1], p2[k], M2);
+  }
+  uint32_t q1[64][9], q2[64][9];
+  for (int k = 0; k < 64; k++)
+    for (int i = 0; i < 9; i++) { q1[k][i] = (uint32_t) p1[k][i]; q2[k][i] = (uint32_t) p2[k][i]; }
+  if (!EZ_CUDA_OK(cudaMemcpyToSymbol(c_mrg_pow1, q1, sizeof(q1))) ||
+      !EZ_CUDA_OK(cudaMemcpyToSymbol(c_mrg_pow2, q2, sizeof(q2))))
+    return EZMOCK_ERR_UNKNOWN;
+  // A^(t*G) for t < MRG_THREADS
+  std::vector<uint32_t> tj(18 * MRG_THREADS);
+  uint64_t g1[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, g2[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  uint64_t s1[9], s2[9];          // A^G
+  memcpy(s1, g1, sizeof(s1));
+  memcpy(s2, g2, sizeof(s2));
+  for (int k = 0; (1 << k) <= MRG_G; k++)
+    if (MRG_G & (1 << k)) { hmat_mul(p1[k], s1, s1, M1); hmat_mul(p2[k], s2, s2, M2); }
+  for (int t = 0; t < MRG_THREADS; t++) {
+    for (int i = 0; i < 9; i++) { tj[18 * t + i] = (uint32_t) g1[i]; tj[18 * t + 9 + i] = (uint32_t) g2[i]; }
+    hmat_mul(s1, g1, g1, M1);
+    hmat_mul(s2, g2, g2, M2);
+  }
+  if (g_mrg_thread_jump) cudaFree(g_mrg_thread_jump);
+  if (!EZ_CUDA_OK(cudaMalloc(&g_mrg_thread_jump, tj.size() * 4)) ||
+      !EZ_CUDA_OK(cudaMemcpy(g_mrg_thread_jump, tj.data(), tj.size() * 4,
+          cudaMemcpyHostToDevice)))
+    return EZMOCK_ERR_MEMORY;
+  g_mrg_dev_ready = dev;
+  return 0;
+}
+
+int mrg_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
+    uint32_t *out) {
+  int e = mrg_prepare(m->device);
+  if (e) return e;
+  uint64_t z = seed, s1[3], s2[3];
+  for (int j = 0; j < 3; j++) s1[j] = splitmix64(&z) % M1;
+  for (int j = 0; j < 3; j++) s2[j] = splitmix64(&z) % M2;
+  if (!s1[0] && !s1[1] && !s1[2]) s1[0] = 1;
+  if (!s2[0] && !s2[1] && !s2[2]) s2[0] = 1;
+  const uint64_t nblk = (count + MRG_BLOCK - 1) / MRG_BLOCK;
+  if (!nblk) return 0;
+  mrg_fill_kernel<<<(unsigned) nblk, MRG_THREADS, 0, m->stream>>>(
+      (uint32_t) s1[0], (uint32_t) s1[1], (uint32_t) s1[2], (uint32_t) s2[0],
+      (uint32_t) s2[1], (uint32_t) s2[2], start, count, g_mrg_thread_jump, out);
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+// ============================================================================
+//                                  MT19937
+// ============================================================================
+
+constexpr int MT_N = 624, MT_M = 397, MT_DEG = 19937, MT_PW = 312;
+constexpr uint32_t MT_A = 0x9908b0dfU, MT_UP = 0x80000000U, MT_LO = 0x7fffffffU;
+constexpr int HW = 6;                                   // Horner window bits
+constexpr int HTAB = 1 << HW;
+constexpr int H_THREADS = 640;
+constexpr int G_THREADS = 640;
+
+__host__ __device__ __forceinline__ uint32_t mt_f(uint32_t a, uint32_t b,
+    uint32_t c) {   // x_{m+624} from x_m (a), x_{m+1} (b), x_{m+397} (c)
+  const uint32_t y = (a & MT_UP) | (b & MT_LO);
+  return c ^ (y >> 1) ^ ((y & 1U) ? MT_A : 0U);
+}
+
+__device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680U;
+  y ^= (y << 15) & 0xefc60000U;
+  y ^= y >> 18;
+  return y;
+}
+
+// Apply p(T) for each polynomial in `plist` (npoly entries, each MT_PW words
+// in `polys`) to state in[in_base + blockIdx.x]; result to out[out_base + b].
+// States are 624-word windows in logical order.
+__global__ void __launch_bounds__(H_THREADS)
+mt_horner_kernel(const uint32_t *__restrict__ states_in, uint32_t *states_out,
+    size_t in_base, size_t out_base, const uint64_t *__restrict__ polys,
+    const int *__restrict__ plist, int npoly) {
+  extern __shared__ uint32_t sm[];
+  uint32_t *tab = sm;                        // HTAB x MT_N
+  uint32_t *ext = tab + HTAB * MT_N;         // MT_N + HW
+  uint32_t *ra = ext + MT_N + HW;            // MT_N
+  uint32_t *rb = ra + MT_N;                  // MT_N
+  const int t = threadIdx.x;
+  const uint32_t *src = states_in + (in_base + blockIdx.x) * MT_N;
+  for (int k = t; k < MT_N; k += blockDim.x) ext[k] = src[k];
+  __syncthreads();
+  for (int ip = 0; ip < npoly; ip++) {
+    const uint64_t *p = polys + (size_t) plist[ip] * MT_PW;
+    if (t < HW) ext[MT_N + t] = mt_f(ext[t], ext[t + 1], ext[MT_M + t]);
+    __syncthreads();
+    for (int e = t; e < HTAB * MT_N; e += blockDim.x) {
+      const int c = e / MT_N, k = e - c * MT_N;
+      uint32_t v = 0;
+#pragma unroll
+      for (int j = 0; j < HW; j++)
+        if (c & (1 << j)) v ^= ext[k + j];
+      tab[e] = v;
+    }
+    for (int k = t; k < MT_N; k += blockDim.x) ra[k] = 0;
+    __syncthreads();
+    uint32_t *r0 = ra, *r1 = rb;
+    const int nwin = (MT_DEG + HW - 1) / HW;
+    for (int q = nwin - 1; q >= 0; q--) {
+      const int b = q * HW;
+      uint64_t bits = p[b >> 6] >> (b & 63);
+      if ((b & 63) + HW > 64 && (b >> 6) + 1 < MT_PW) bits |= p[(b >> 6) + 1] << (64 - (b & 63));
+      const int c = (int) (bits & (HTAB - 1));
+      const uint32_t *tc = tab + c * MT_N;
+      if (t < MT_N) {
+        uint32_t v;
+        if (t < MT_N - HW) v = r0[t + HW];
+        else {
+          const int s = t - (MT_N - HW);
+          v = mt_f(r0[s], r0[s + 1], r0[MT_M + s]);
+        }
+        r1[t] = v ^ tc[t];
+      }
+      __syncthreads();
+      uint32_t *tmp = r0; r0 = r1; r1 = tmp;
+    }
+    for (int k = t; k < MT_N; k += blockDim.x) ext[k] = r0[k];
+    __syncthreads();
+  }
+  uint32_t *dst = states_out + (out_base + blockIdx.x) * MT_N;
+  for (int k = t; k < MT_N; k += blockDim.x) dst[k] = ext[k];
+}
+
+// Block c generates draws [c*L, min((c+1)*L, count)) from window states[c].
+__global__ void __launch_bounds__(G_THREADS)
+mt_gen_kernel(const uint32_t *__restrict__ states, uint64_t L, uint64_t count,
+    uint32_t *__restrict__ out) {
+  __shared__ uint32_t wa[MT_N], wb[MT_N];
+  const int t = threadIdx.x;
+  const uint64_t c0 = (uint64_t) blockIdx.x * L;
+  if (c0 >= count) return;
+  const uint64_t c1 = (c0 + L < count) ? c0 + L : count;
+  for (int k = t; k < MT_N; k += blockDim.x) wa[k] = states[(size_t) blockIdx.x * MT_N + k];
+  __syncthreads();
+  uint32_t *o = wa, *n = wb;
+  for (uint64_t g = c0; g < c1; g += MT_N) {
+    // x_{m+624+t} = x_{m+397+t} ^ f(x_{m+t}, x_{m+t+1}), in three phases
+    if (t < 227) n[t] = mt_f(o[t], o[t + 1], o[MT_M + t]);
+    __syncthreads();
+    if (t >= 227 && t < 454) n[t] = mt_f(o[t], o[t + 1], n[t - 227]);
+    __syncthreads();
+    if (t >= 454 && t < MT_N)
+      n[t] = mt_f(o[t], (t + 1 < MT_N) ? o[t + 1] : n[0], n[t - 227]);
+    __syncthreads();
+    if (t < MT_N && g + t < c1) out[g + t] = mt_temper(n[t]);
+    uint32_t *tmp = o; o = n; n = tmp;
+    __syncthreads();
+  }
+}
+
+// ---- host: characteristic polynomial and x^(2^k) table ----
+inline int hbit(const uint64_t *a, long b) { return (int) ((a[b >> 6] >> (b & 63)) & 1ULL); }
+
+struct MtTables {
+  bool ok = false;
+  std::vector<uint64_t> phi;                 // MT_PW + 1 words
+  std::vector<uint64_t> xpow;                // 64 x MT_PW
+};
+
+void mt_seed_window(uint64_t seed, uint32_t *w) {
+  if (seed <= 0xffffffffULL) {
+    w[0] = (uint32_t) seed;
+    for (int i = 1; i < MT_N; i++) w[i] = 1812433253U * (w[i - 1] ^ (w[i - 1] >> 30)) + (uint32_t) i;
+    return;
+  }
+  const uint32_t key[2] = {(uint32_t) seed, (uint32_t) (seed >> 32)};
+  w[0] = 19650218U;
+  for (int i = 1; i < MT_N; i++) w[i] = 1812433253U * (w[i - 1] ^ (w[i - 1] >> 30)) + (uint32_t) i;
+  int i = 1, j = 0;
+  for (int k = MT_N; k; k--) {
+    w[i] = (w[i] ^ ((w[i - 1] ^ (w[i - 1] >> 30)) * 1664525U)) + key[j] + (uint32_t) j;
+    i++; j++;
+    if (i >= MT_N) { w[0] = w[MT_N - 1]; i = 1; }
+    if (j >= 2) j = 0;
+  }
+  for (int k = MT_N - 1; k; k--) {
+    w[i] = (w[i] ^ ((w[i - 1] ^ (w[i - 1] >> 30)) * 1566083941U)) - (uint32_t) i;
+    i++;
+    if (i >= MT_N) { w[0] = w[MT_N - 1]; i = 1; }
+  }
+  w[0] = 0x80000000U;
+}
+
+void build_mt_tables(MtTables &T) {
+  // Berlekamp-Massey on the top bit of the raw words of one stream.
+  const long len = 2L * MT_DEG + 128;
+  const long nw = (len + 63) / 64 + 2;
+  std::vector<uint64_t> rev(nw, 0), C(nw, 0), B(nw, 0), Tt(nw, 0);
+  {
+    std::vector<uint32_t> w(MT_N);
+    mt_seed_window(5489U, w.data());
+    int pos = 0;
+    for (long n = 0; n < len; n++) {
+      const int p1 = (pos + 1) % MT_N, pm = (pos + MT_M) % MT_N;
+      const uint32_t x = mt_f(w[pos], w[p1], w[pm]);
+      w[pos] = x;
+      pos = p1;
+      const long tpos = len - 1 - n;
+      if (x >> 31) rev[tpos >> 6] |= 1ULL << (tpos & 63);
+    }
+  }
+  C[0] = B[0] = 1;
+  long L = 0, m = 1;
+  auto add_shift = [&](std::vector<uint64_t> &dst, const std::vector<uint64_t> &src, long sh) {
+    const long ws = sh >> 6, bs = sh & 63;
+    for (long w = nw - 1; w >= 0; w--) {
+      uint64_t v = 0;
+      if (w - ws >= 0) v = src[w - ws] << bs;
+      if (bs && w - ws - 1 >= 0) v |= src[w - ws - 1] >> (64 - bs);
+      dst[w] ^= v;
+    }
+  };
+  for (long n = 0; n < len; n++) {
+    const long o = len - 1 - n;
+    const long lw = L / 64 + 1;
+    uint64_t acc = 0;
+    for (long w = 0; w < lw; w++) {
+      const long b = o + 64 * w, bw = b >> 6, bs = b & 63;
+      uint64_t v = rev[bw] >> bs;
+      if (bs && bw + 1 < nw) v |= rev[bw + 1] << (64 - bs);
+      acc ^= C[w] & v;
+    }
+    if (!__builtin_parityll(acc)) { m++; continue; }
+    if (2 * L <= n) {
+      Tt = C;
+      add_shift(C, B, m);
+      L = n + 1 - L;
+      B = Tt;
+      m = 1;
+    }
+    else { add_shift(C, B, m); m++; }
+  }
+  if (L != MT_DEG) return;
+  T.phi.assign(MT_PW + 1, 0);
+  for (long j = 0; j <= L; j++)
+    if (hbit(C.data(), L - j)) T.phi[j >> 6] |= 1ULL << (j & 63);
+  // phi << s for s < 64
+  std::vector<uint64_t> sh(64 * (MT_PW + 2), 0);
+  for (int s = 0; s < 64; s++)
+    for (int w = 0; w <= MT_PW; w++) {
+      sh[s * (MT_PW + 2) + w] ^= T.phi[w] << s;
+      if (s) sh[s * (MT_PW + 2) + w + 1] ^= T.phi[w] >> (64 - s);
+    }
+  auto spread = [](uint32_t v) {
+    uint64_t x = v;
+    x = (x | (x << 16)) & 0x0000ffff0000ffffULL;
+    x = (x | (x << 8)) & 0x00ff00ff00ff00ffULL;
+    x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0fULL;
+    x = (x | (x << 2)) & 0x3333333333333333ULL;
+    x = (x | (x << 1)) & 0x5555555555555555ULL;
+    return x;
+  };
+  T.xpow.assign(64 * MT_PW, 0);
+  T.xpow[0] = 2;                                         // x
+  std::vector<uint64_t> r(2 * MT_PW + 4);
+  for (int k = 1; k < 64; k++) {
+    std::fill(r.begin(), r.end(), 0);
+    const uint64_t *prev = &T.xpow[(k - 1) * MT_PW];
+    for (int w = 0; w < MT_PW; w++) {
+      r[2 * w] = spread((uint32_t) prev[w]);
+      r[2 * w + 1] = spread((uint32_t) (prev[w] >> 32));
+    }
+    for (long b = 2L * MT_DEG; b >= MT_DEG; b--) {
+      if (!hbit(r.data(), b)) continue;
+      const long t = b - MT_DEG, ws = t >> 6;
+      const uint64_t *ph = &sh[(t & 63) * (MT_PW + 2)];
+      for (long w = 0; w < MT_PW + 2 && ws + w < (long) r.size(); w++) r[ws + w] ^= ph[w];
+    }
+    memcpy(&T.xpow[k * MT_PW], r.data(), MT_PW * sizeof(uint64_t));
+  }
+  T.ok = true;
+}
+
+std::mutex g_mt_mu;
+MtTables g_mt;
+bool g_mt_built = false;
+int g_mt_dev_ready = -1;
+uint64_t *g_mt_xpow_dev = nullptr;
+
+int mt_prepare(int dev) {
+  std::lock_guard<std::mutex> lk(g_mt_mu);
+  if (!g_mt_built) { build_mt_tables(g_mt); g_mt_built = true; }
+  if (!g_mt.ok) return EZMOCK_ERR_RNG_SET;
+  if (g_mt_dev_ready == dev) return 0;
+  if (g_mt_xpow_dev) cudaFree(g_mt_xpow_dev);
+  if (!EZ_CUDA_OK(cudaMalloc(&g_mt_xpow_dev, g_mt.xpow.size() * 8)) ||
+      !EZ_CUDA_OK(cudaMemcpy(g_mt_xpow_dev, g_mt.xpow.data(), g_mt.xpow.size() * 8,
+          cudaMemcpyHostToDevice)))
+    return EZMOCK_ERR_MEMORY;
+  if (!EZ_CUDA_OK(cudaFuncSetAttribute(mt_horner_kernel,
+          cudaFuncAttributeMaxDynamicSharedMemorySize,
+          (int) ((HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t)))))
+    return EZMOCK_ERR_UNKNOWN;
+  g_mt_dev_ready = dev;
+  return 0;
+}
+
+int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
+    uint32_t *out) {
+  if (!count) return 0;
+  int e = mt_prepare(m->device);
+  if (e) return e;
+  // chunk length L = 2^l and number of chunks P = 2^p with P*L >= count
+  int l = 12, p = 0;
+  while ((1ULL << l) * 256ULL < count && l < 40) l++;
+  while (((uint64_t) 1 << (l + p)) < count) p++;
+  const uint64_t L = 1ULL << l;
+  const uint64_t P = 1ULL << p;
+  // scratch: P states + seed state + polynomial index list
+  std::vector<int> plist;
+  for (int k = 0; k < 64; k++)
+    if ((start >> k) & 1ULL) plist.push_back(k);
+  for (int lev = 0; lev < p; lev++) plist.push_back(l + lev);
+  const size_t st_bytes = (size_t) (P + 1) * MT_N * sizeof(uint32_t);
+  const size_t need = st_bytes + plist.size() * sizeof(int) + 256;
+  if ((e = ez_rng_scratch(m, need))) return e;
+  uint32_t *states = (uint32_t *) m->rng_scratch;    // [0]: seed, [1..P]: chunks
+  int *d_plist = (int *) ((char *) m->rng_scratch + st_bytes);
+  std::vector<uint32_t> w(MT_N);
+  mt_seed_window(seed, w.data());
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(states, w.data(), MT_N * 4, cudaMemcpyHostToDevice, m->stream)) ||
+      !EZ_CUDA_OK(cudaMemcpyAsync(d_plist, plist.data(), plist.size() * sizeof(int),
+          cudaMemcpyHostToDevice, m->stream)))
+    return EZMOCK_ERR_UNKNOWN;
+  const size_t smem = (HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t);
+  const int nbase = (int) plist.size() - p;
+  // chunk 0 (state index 1) = jump of the seed window to `start`
+  if (nbase > 0)
+    mt_horner_kernel<<<1, H_THREADS, smem, m->stream>>>(states, states, 0, 1,
+        g_mt_xpow_dev, d_plist, nbase);
+  else
+    cudaMemcpyAsync(states + MT_N, states, MT_N * 4, cudaMemcpyDeviceToDevice, m->stream);
+  for (int lev = 0; lev < p; lev++) {
+    const unsigned nb = 1u << lev;
+    mt_horner_kernel<<<nb, H_THREADS, smem, m->stream>>>(states, states, 1,
+        1 + nb, g_mt_xpow_dev, d_plist + nbase + lev, 1);
+  }
+  mt_gen_kernel<<<(unsigned) P, G_THREADS, 0, m->stream>>>(states + MT_N, L,
+      count, out);
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+// Host copy of the seeding, used for the MT19937 raw-output check below.
+}  // namespace
+
+int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
+    uint64_t count, uint32_t *out) {
+  if (ran == EZMOCK_RNG_MT19937) return mt_fill(m, seed, start, count, out);
+  return mrg_fill(m, seed, start, count, out);
+}

@@ -1,0 +1,59 @@
+/*
+ * ezmock_b200.h -- extensions of the B200 EZmock engine.
+ *
+ * These entry points have no counterpart in the reference's libEZmock; they
+ * expose GPU-side controls and data for tests, benchmarks and callers that
+ * keep the catalogue on the GPU.  All follow the sticky-error convention of
+ * EZmock.h and return an EZmock error code.
+ */
+#ifndef EZMOCK_B200_EXT_H
+#define EZMOCK_B200_EXT_H
+
+#include "EZmock.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Options for EZmockB200_set_option. */
+#define EZMOCKB200_OPT_CIC_MODE 1   /* 0: float atomics (default), 1: deterministic */
+#define EZMOCKB200_OPT_TIMING   2   /* 1: record per-stage CUDA-event timings */
+#define EZMOCKB200_OPT_DEVICE   3   /* CUDA device ordinal (before the first field) */
+
+int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
+    int *err);
+
+/* Stage timings (milliseconds, CUDA events on the instance stream) of the
+   most recent create/populate calls, in the order: rng, ic, fft_i, fft_j,
+   fft_k, cic, bias, select, emit, vel, d2h.  Returns the number written. */
+int EZmockB200_stage_times(EZMOCK *ez, double *ms, const int n);
+
+/* Copies a device field to host memory (Ngrid^3 `real` values):
+   0..2 psi_x,y,z; 3 rho; 4..6 CIC-painted displacements (un-normalised). */
+int EZmockB200_copy_field(EZMOCK *ez, const int which, real *out, int *err);
+
+/* EZmock_populate_tracer without the device-to-host copy: the catalogue
+   stays in GPU memory (read it with EZmockB200_copy_catalog). */
+int EZmockB200_populate_device(EZMOCK *ez, const real *params,
+    const size_t nexp, size_t *ntracer, int *err);
+
+/* Copies the last device catalogue (n = its length) into six host arrays. */
+int EZmockB200_copy_catalog(EZMOCK *ez, real *x, real *y, real *z, real *vx,
+    real *vy, real *vz, const size_t n, int *err);
+
+/* Raw 32-bit draws [start, start+count) of stream `seed` generated on the
+   GPU (0: MRG32k3a, 1: MT19937). */
+int EZmockB200_rng_raw(const int randgen, const uint64_t seed,
+    const uint64_t start, const uint64_t count, uint32_t *out);
+
+/* Waits for all work of the instance. */
+int EZmockB200_sync(EZMOCK *ez);
+
+/* Size in bytes of `real` in this build (4 or 8). */
+int EZmockB200_real_size(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
