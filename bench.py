@@ -1,0 +1,361 @@
+"""Benchmark: seconds per EZmock mock on B200 (create_dens_field + populate).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one mock of the single-mock workload (Ngrid 512^3, box 2500 Mpc/h,
+n = 2e-4 (h/Mpc)^3, rho_c 0.8, rho_exp 20, pdf_base 0.3, sigma_v 400 km/s,
+synthetic BBKS P(k) with sigma_8 = 0.81, z = 0.8, MT19937) through the C-ABI
+library: the initial field, three Zel'dovich displacement FFTs, the CIC
+density and the tracer population.  With N > 1 (torchrun, one process per
+GPU) every rank produces its own mocks (independent seeds; replicas, weak
+scaling) and the slowest rank's device time defines the job time.
+
+The JSON line reports
+  value      : s/mock with inputs resident on the GPU (catalogue left on the
+               GPU), from CUDA events on the library's stream, max over ranks;
+  e2e        : s/mock through the public EZmock_* calls with host buffers
+               (P(k) upload, catalogue copied into malloc'd host arrays);
+  roofline   : the dominant kernel's algorithmic bytes / launch time against
+               the measured HBM copy bandwidth;
+  cpu_baseline (rank 0, N = 1): the reference's own libEZmock sources
+               (oracle/_ref, OpenMP, all host cores) on the same workload.
+`--impl reference` runs only that CPU path and prints its line.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s/mock at 512^3 (FP32 production mode)"
+STAGES = ["rng", "ic", "fft_i", "fft_j", "fft_k", "cic", "bias", "select", "emit", "vel",
+          "d2h"]
+
+
+def workload_desc(cfg):
+    return (f"{cfg.name}: 1 mock {cfg.Ng}^3, box {cfg.Lbox:g} Mpc/h, n={cfg.n_tracer:g}, "
+            f"rho_c={cfg.rho_c:g}, rho_exp={cfg.rho_exp:g}, pdf_base={cfg.pdf_base:g}, "
+            f"sigma_v={cfg.sigma_v:g}, {'MT19937' if cfg.rng else 'MRG32k3a'}, z={cfg.z:g}")
+
+
+def pk_trim_len(k, Ng, Lbox):
+    """Number of P(k) bins the library keeps (linear_pk.c:114-126)."""
+    kmin = 2 * math.pi / Lbox
+    kmax = math.pi * Ng / Lbox * math.sqrt(3)
+    imin = int(np.searchsorted(k, kmin, side="right"))
+    imax = int(np.searchsorted(k, kmax, side="right"))
+    imin = max(imin - 3, 0)
+    imax = min(imax + 3, len(k))
+    return imax - imin
+
+
+def algorithmic_bytes(Ng, b):
+    """Compulsory HBM bytes per launch of each stage (FP32: b = 4)."""
+    N = Ng ** 3
+    Nk = Ng * Ng * (Ng // 2 + 1)
+    H = Nk * 2 * b                               # one half-complex spectrum
+    return {
+        "ic": 2 * Nk * 4 + H,                    # draws read, spectrum written
+        "fft_i": 3 * H,                          # read S, write 2 spectra
+        "fft_j": 5 * H,                          # read 2, write 3
+        "fft_k": 3 * H + 3 * N * b,              # read 3 spectra, write 3 psi
+        "cic": 3 * N * b + 4 * N * b,            # read psi, write rho + 3 momenta
+    }
+
+
+def read_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic():
+    """Per-launch DRAM bytes of each kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(cfg, k, P, steps, warmup, allow_scale=True):
+    """The reference's libEZmock (oracle/_ref, OpenMP, all host threads) on the
+    workload; returns (s/mock, sample description, threads)."""
+    from oracle.pyoracle import RefLib
+    R = RefLib(32, nthread=0)
+    nthreads = os.cpu_count()
+
+    def one(Ng, Lbox, seed):
+        m = R.new(Lbox, Ng, cfg.rng, seed)
+        m.eval_growth(cfg.z, cfg.omega_m)
+        m.setup_pk(k, P)
+        t0 = time.perf_counter()
+        m.create()
+        m.populate(cfg.params(), int(round(cfg.n_tracer * Lbox ** 3)))
+        return time.perf_counter() - t0
+
+    # a 256^3 probe decides whether full-size steps fit in a few minutes
+    ng_s = cfg.Ng // 2
+    t_small = one(ng_s, cfg.Lbox / 2, 1)
+    est = t_small * 8 * math.log(cfg.Ng ** 3) / math.log(ng_s ** 3)
+    if est * (steps + min(warmup, 1)) < 240 or not allow_scale:
+        for w in range(min(warmup, 1)):
+            one(cfg.Ng, cfg.Lbox, 1000 + w)
+        ts = [one(cfg.Ng, cfg.Lbox, 1 + s) for s in range(steps)]
+        return (statistics.median(ts), f"{steps} full {cfg.Ng}^3 mocks (median), "
+                f"{nthreads} OpenMP threads", nthreads)
+    ts = [one(ng_s, cfg.Lbox / 2, 1 + s) for s in range(steps)]
+    scale = 8 * math.log(cfg.Ng ** 3) / math.log(ng_s ** 3)
+    return (statistics.median(ts) * scale,
+            f"{steps} mocks at {ng_s}^3 (median) x {scale:.2f} (N log N scaling to "
+            f"{cfg.Ng}^3), {nthreads} OpenMP threads", nthreads)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="single512")
+    ap.add_argument("--rng", type=int, default=None, help="0 MRG32k3a, 1 MT19937")
+    ap.add_argument("--prec", type=int, default=32)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    from ezmock_b200.workloads import CONFIGS, bbks_pk
+    cfg = CONFIGS[args.workload]
+    if args.rng is not None:
+        cfg.rng = args.rng
+    k, P = bbks_pk()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n_gpus = max(world, 1)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        try:
+            v, sample, cores = cpu_reference(cfg, k, P, args.steps, args.warmup)
+        except Exception as e:             # the reference build is missing
+            print(json.dumps({"impl": "reference", "unavailable": f"reference build: {e}"}))
+            return 0
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "s/mock",
+            "n_gpus": n_gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic BBKS P(k)",
+            "config": {"workload": workload_desc(cfg), "Ngrid": cfg.Ng, "Lbox": cfg.Lbox},
+            "cpu_baseline": {"value": v, "unit": "s/mock", "cores": cores, "kind": "reference",
+                             "sample": sample + "; FFT: project CPU FFT (FFTW3 not installed)"},
+            "e2e": {"value": v, "unit": "s/mock", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return 0
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from ezmock_b200 import EZmock
+    m = EZmock(Lbox=cfg.Lbox, Ngrid=cfg.Ng, rng=cfg.rng, seed=1 + rank * 100000,
+               prec=args.prec)
+    L = m._L
+    m.set_option(3, local)            # device
+    m.set_option(2, 1)                # stage timings
+    m.eval_growth_params(cfg.z, cfg.omega_m)
+    m.setup_linear_pk(k, P)
+    nexp = cfg.nexp
+    params = cfg.params()
+    b = 4 if args.prec == 32 else 8
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def reduce_max(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    seed = [1 + rank * 100000]
+
+    def device_step():
+        seed[0] += 1
+        m.set_option(4, seed[0])
+        m.create_dens_field_from_ic()
+        stage_c = m.stage_times()
+        n = m.populate_device(*params, nexp)
+        return n, stage_c
+
+    for _ in range(args.warmup):
+        device_step()
+    m.sync()
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    l0 = L.EZmockB200_launch_count()
+    L.EZmockB200_mark(m._ez, 0)
+    t0 = time.perf_counter()
+    stage_acc = {s: [] for s in STAGES}
+    ntr = 0
+    for _ in range(args.steps):
+        ntr, st_c = device_step()
+        st_p = m.stage_times()
+        for s in STAGES:
+            v = st_p[s] if s not in ("rng", "ic", "fft_i", "fft_j", "fft_k", "cic") else st_c[s]
+            if v >= 0:
+                stage_acc[s].append(v)
+    L.EZmockB200_mark(m._ez, 1)
+    ms = ctypes.c_double()
+    L.EZmockB200_elapsed(m._ez, 0, 1, ctypes.byref(ms))
+    wall = time.perf_counter() - t0
+    launches = L.EZmockB200_launch_count() - l0
+    clocks = clk.stop()
+    barrier()
+    t_dev = reduce_max(ms.value / 1e3)
+    value = t_dev / (n_gpus * args.steps)
+
+    # end to end through the public API with host buffers
+    barrier()
+    L.EZmockB200_mark(m._ez, 2)
+    te0 = time.perf_counter()
+    for s in range(args.steps):
+        seed[0] += 1
+        m.set_option(4, seed[0])
+        m.setup_linear_pk(k, P)               # P(k) table uploaded by the next call
+        m.create_dens_field_from_ic()
+        cat = m.populate_tracer(*params, nexp)
+    L.EZmockB200_mark(m._ez, 3)
+    e2e_wall = time.perf_counter() - te0
+    ems = ctypes.c_double()
+    L.EZmockB200_elapsed(m._ez, 2, 3, ctypes.byref(ems))
+    e2e = reduce_max(max(ems.value / 1e3, e2e_wall)) / (n_gpus * args.steps)
+    h2d = 3 * pk_trim_len(k, cfg.Ng, cfg.Lbox) * 8
+    d2h = 6 * len(cat[0]) * b
+
+    # roofline of the dominant kernel
+    peak, peak_kind = read_peak()
+    algo = algorithmic_bytes(cfg.Ng, b)
+    med = {s: statistics.median(v) for s, v in stage_acc.items() if v}
+    stages_gbs = {s: {"ms": round(med[s], 4),
+                      "GB/s": round(algo[s] / (med[s] * 1e-3) / 1e9, 1) if s in algo else None}
+                  for s in med}
+    dom = max((s for s in algo if s in med), key=lambda s: med[s])
+    achieved = algo[dom] / (med[dom] * 1e-3) / 1e9
+    traffic = read_traffic().get(dom)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "algorithmic_bytes": algo[dom]}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "s/mock", "n_gpus": n_gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev * 1e3 / args.steps,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.prec == 32 else "f64",
+        "data": "synthetic (BBKS P(k), sigma_8 = 0.81)",
+        "config": {"workload": workload_desc(cfg), "Ngrid": cfg.Ng, "Lbox": cfg.Lbox,
+                   "nexp": nexp, "ntracer": ntr, "parallelism": f"replicas x{n_gpus}",
+                   "l2": "inputs larger than L2 (psi 1.6 GB, spectra 1.7 GB per mock)"},
+        "e2e": {"value": e2e, "unit": "s/mock", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches, "roofline": roof, "stages": stages_gbs,
+        "clocks": clocks, "wall_s_per_mock": wall / args.steps,
+    }
+    if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
+        try:
+            v, sample, cores = cpu_reference(cfg, k, P, 1, 0)
+            line["cpu_baseline"] = {"value": v, "unit": "s/mock", "cores": cores,
+                                    "kind": "reference",
+                                    "sample": sample + "; FFT: project CPU FFT "
+                                    "(FFTW3 not installed)"}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unit": "s/mock", "cores": None,
+                                    "kind": "reference", "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -73,6 +73,8 @@ def load(prec=32):
     L.EZmockB200_populate_device.argtypes = [_vp, _vp, ctypes.c_size_t, _sp, _ip]
     L.EZmockB200_copy_catalog.restype = ctypes.c_int
     L.EZmockB200_copy_catalog.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _ip]
+    L.EZmockB200_select_counts.restype = ctypes.c_int
+    L.EZmockB200_select_counts.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int, _sp, _sp, _vp, _ip]
     L.EZmockB200_rng_raw.restype = ctypes.c_int
     L.EZmockB200_rng_raw.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
                                      ctypes.c_uint64, _vp]
@@ -80,6 +82,13 @@ def load(prec=32):
     L.EZmockB200_sync.argtypes = [_vp]
     L.EZmockB200_real_size.restype = ctypes.c_int
     L.EZmockB200_real_size.argtypes = []
+    L.EZmockB200_launch_count.restype = ctypes.c_longlong
+    L.EZmockB200_launch_count.argtypes = []
+    L.EZmockB200_mark.restype = ctypes.c_int
+    L.EZmockB200_mark.argtypes = [_vp, ctypes.c_int]
+    L.EZmockB200_elapsed.restype = ctypes.c_int
+    L.EZmockB200_elapsed.argtypes = [_vp, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_double)]
     L._rt = rt
     _cache[prec] = L
     return L

@@ -158,9 +158,9 @@ int ez_cic(EzMesh *m, double Lbox) {
     unsigned long long *acc = m->fixacc;
     if (!EZ_CUDA_OK(cudaMemsetAsync(acc, 0, need, m->stream))) return EZMOCK_ERR_UNKNOWN;
     cic_fixed_kernel<<<grid, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
-        m->psi[2], acc, Ng, igs, N);
+        m->psi[2], acc, Ng, igs, N); ez_count_launch();
     fixed_to_real<<<grid, CIC_NT, 0, m->stream>>>(acc, m->rho, m->paint[0],
-        m->paint[1], m->paint[2], N);
+        m->paint[1], m->paint[2], N); ez_count_launch();
   }
   else {
     if (!EZ_CUDA_OK(cudaMemsetAsync(m->rho, 0, N * sizeof(real), m->stream))) return EZMOCK_ERR_UNKNOWN;
@@ -168,7 +168,7 @@ int ez_cic(EzMesh *m, double Lbox) {
       if (!EZ_CUDA_OK(cudaMemsetAsync(m->paint[d], 0, N * sizeof(real), m->stream)))
         return EZMOCK_ERR_UNKNOWN;
     cic_atomic_kernel<true><<<grid, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
-        m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, N);
+        m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, N); ez_count_launch();
   }
   ez_stage_end(m, ST_CIC);
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;

@@ -469,17 +469,17 @@ int ez_fft_c2r_psi(EzMesh *m) {
   const int nkt = (m->Nk + K - 1) / K;
   ez_stage_begin(m, ST_FFT_I);
   fft_pass_i<<<dim3(Ng, nkt), FFT_NT, sm_i, m->stream>>>(m->spec[0], m->spec[1],
-      m->spec[2], Ng, Nkp, K, pn);
+      m->spec[2], Ng, Nkp, K, pn); ez_count_launch();
   ez_stage_end(m, ST_FFT_I);
   ez_stage_begin(m, ST_FFT_J);
   fft_pass_j<<<dim3(Ng, nkt), FFT_NT, sm_j, m->stream>>>(m->spec[0], m->spec[1],
-      m->spec[2], Ng, Nkp, K, pn);
+      m->spec[2], Ng, Nkp, K, pn); ez_count_launch();
   ez_stage_end(m, ST_FFT_J);
   const size_t nrows = (size_t) Ng * Ng;
   ez_stage_begin(m, ST_FFT_K);
   fft_pass_k<<<(unsigned) ((nrows + R - 1) / R), FFT_NT, sm_k, m->stream>>>(
       m->spec[0], m->spec[1], m->spec[2], m->psi[0], m->psi[1], m->psi[2], Ng,
-      Nkp, R, nrows, ph, twg);
+      Nkp, R, nrows, ph, twg); ez_count_launch();
   ez_stage_end(m, ST_FFT_K);
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
@@ -506,14 +506,14 @@ int ez_fft_r2c_delta(EzMesh *m, const real *d_delta) {
   }
   const size_t nrows = (size_t) Ng * Ng;
   fft_r2c_rows<<<(unsigned) ((nrows + R - 1) / R), FFT_NT, sm_r, m->stream>>>(
-      d_delta, m->spec[0], Ng, Nkp, R, nrows, ph, twg);
+      d_delta, m->spec[0], Ng, Nkp, R, nrows, ph, twg); ez_count_launch();
   const int nkt = (m->Nk + K - 1) / K;
-  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, m->stream>>>(m->spec[0], Ng, Nkp, K, 1, pn);
-  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, m->stream>>>(m->spec[0], Ng, Nkp, K, 0, pn);
+  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, m->stream>>>(m->spec[0], Ng, Nkp, K, 1, pn); ez_count_launch();
+  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, m->stream>>>(m->spec[0], Ng, Nkp, K, 0, pn); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
 int ez_scale_psi(EzMesh *m, real f) {
-  scale_kernel<<<148 * 16, 256, 0, m->stream>>>(m->psi[0], 3 * m->N, f);
+  scale_kernel<<<148 * 16, 256, 0, m->stream>>>(m->psi[0], 3 * m->N, f); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }

@@ -8,6 +8,7 @@
 #include "ez_internal.cuh"
 #include "ezmock_b200.h"
 
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -149,6 +150,7 @@ void mesh_free_device(EzMesh *m) {
   if (m->h_stage) cudaFreeHost(m->h_stage);
   if (m->stream) cudaStreamDestroy(m->stream);
   for (int i = 0; i < 2 * ST_NSTAGE; i++) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
+  for (int i = 0; i < 8; i++) if (m->mark[i]) cudaEventDestroy(m->mark[i]);
 }
 
 int set_device(EzMesh *m) {
@@ -240,6 +242,9 @@ int run_populate(EZMOCK *ez, const real *params, size_t nexp, bool att_part,
 }
 
 }  // namespace
+
+static std::atomic<long long> g_launches(0);
+void ez_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // ============================================================================
 //                       memory management (used by stages)
@@ -748,6 +753,10 @@ int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
       if (m->spec[0] || value < 0) return (*err = EZMOCK_ERR_ARG_PARAMS);
       m->device = (int) value;
       return 0;
+    case EZMOCKB200_OPT_SEED:
+      if (value <= 0) return (*err = EZMOCK_ERR_ARG_SEED);
+      RNG(ez)->seed = (uint64_t) value;
+      return 0;
     default: return (*err = EZMOCK_ERR_ARG_PARAMS);
   }
 }
@@ -805,16 +814,41 @@ int EZmockB200_copy_catalog(EZMOCK *ez, real *x, real *y, real *z, real *vx,
   if (*err != EZMOCK_SUCCESS) return *err;
   if (!ez) return (*err = EZMOCK_ERR_ARG_EZ);
   EzMesh *m = MESH(ez);
-  if (!m->cat || n > m->cat_cap) return (*err = EZMOCK_ERR_ARG_NDATA);
+  if (!m->cat || n != m->cat_n) return (*err = EZMOCK_ERR_ARG_NDATA);
   real *dst[6] = {x, y, z, vx, vy, vz};
   cudaSetDevice(m->device);
   for (int i = 0; i < 6; i++) {
     if (!dst[i]) return (*err = EZMOCK_ERR_ARG_NULL);
-    if (!EZ_CUDA_OK(cudaMemcpyAsync(dst[i], m->cat + (size_t) i * m->cat_cap, n * sizeof(real),
+    if (!EZ_CUDA_OK(cudaMemcpyAsync(dst[i], m->cat + (size_t) i * n, n * sizeof(real),
             cudaMemcpyDeviceToHost, m->stream)))
       return (*err = EZMOCK_ERR_UNKNOWN);
   }
   if (!EZ_CUDA_OK(cudaStreamSynchronize(m->stream))) return (*err = EZMOCK_ERR_UNKNOWN);
+  return 0;
+}
+
+int EZmockB200_select_counts(EZMOCK *ez, const real *rhot,
+    const size_t *hist, size_t *pdf, const int nmax, size_t *ncell,
+    size_t *ntot, int16_t *nt, int *err) {
+  if (!err) return EZMOCK_ERR_ARG_ECODE;
+  if (*err != EZMOCK_SUCCESS) return *err;
+  if (!ez) return (*err = EZMOCK_ERR_ARG_EZ);
+  if (!rhot || !hist || !pdf || !ncell || !ntot || !nt) return (*err = EZMOCK_ERR_ARG_NULL);
+  if (nmax <= 0 || nmax > EZ_MAX_NT) return (*err = EZMOCK_ERR_ARG_PARAMS);
+  EzMesh *m = MESH(ez);
+  if (!m->have_field) return (*err = EZMOCK_ERR_ARG_MESH);
+  cudaSetDevice(m->device);
+  unsigned long long h[EZ_NLOGB];
+  for (int i = 0; i < EZ_NLOGB; i++) h[i] = hist[i];
+  // staging for the counts: the draw buffer holds >= Ngrid^3 32-bit words
+  int16_t *d_nt = (int16_t *) m->draws;
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(m->spec[0], rhot, m->N * sizeof(real), cudaMemcpyHostToDevice, m->stream)))
+    return (*err = EZMOCK_ERR_UNKNOWN);
+  int e = ez_select_counts(m, h, pdf, nmax, ncell, ntot, d_nt);
+  if (e) return (*err = e);
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(nt, d_nt, m->N * sizeof(int16_t), cudaMemcpyDeviceToHost, m->stream)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
+    return (*err = EZMOCK_ERR_UNKNOWN);
   return 0;
 }
 
@@ -849,5 +883,29 @@ int EZmockB200_sync(EZMOCK *ez) {
 }
 
 int EZmockB200_real_size(void) { return (int) sizeof(real); }
+
+long long EZmockB200_launch_count(void) { return g_launches.load(); }
+
+int EZmockB200_mark(EZMOCK *ez, const int slot) {
+  if (!ez || slot < 0 || slot >= 8) return EZMOCK_ERR_ARG_PARAMS;
+  EzMesh *m = MESH(ez);
+  if (m->device < 0 || !m->stream) return EZMOCK_ERR_ARG_MESH;
+  cudaSetDevice(m->device);
+  if (!m->mark[slot] && !EZ_CUDA_OK(cudaEventCreate(&m->mark[slot]))) return EZMOCK_ERR_UNKNOWN;
+  return EZ_CUDA_OK(cudaEventRecord(m->mark[slot], m->stream)) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+int EZmockB200_elapsed(EZMOCK *ez, const int a, const int b, double *ms) {
+  if (!ez || !ms || a < 0 || a >= 8 || b < 0 || b >= 8) return EZMOCK_ERR_ARG_PARAMS;
+  EzMesh *m = MESH(ez);
+  if (!m->mark[a] || !m->mark[b]) return EZMOCK_ERR_ARG_PARAMS;
+  cudaSetDevice(m->device);
+  float t = 0;
+  if (!EZ_CUDA_OK(cudaEventSynchronize(m->mark[b])) ||
+      !EZ_CUDA_OK(cudaEventElapsedTime(&t, m->mark[a], m->mark[b])))
+    return EZMOCK_ERR_UNKNOWN;
+  *ms = t;
+  return 0;
+}
 
 }  // extern "C"

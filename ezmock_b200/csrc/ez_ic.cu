@@ -137,7 +137,7 @@ int ez_ic_spectrum(EzMesh *m, const EzPk *pk, double Lbox, int ran,
   ez_stage_begin(m, ST_IC);
   ic_kernel<<<(unsigned) ((size_t) Ng * Ng), IC_NT, 0, m->stream>>>(
       m->spec[0], draws, pk->d_tab, pk->n, pk->log ? 1 : 0, Ng, m->Nk, m->Nkp,
-      kfac, logkfac, Pfac, ran, fixamp, iphase);
+      kfac, logkfac, Pfac, ran, fixamp, iphase); ez_count_launch();
   ez_stage_end(m, ST_IC);
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
@@ -147,6 +147,6 @@ int ez_wn_scale(EzMesh *m, const EzPk *pk, double Lbox) {
   const double kfac = EZ_PI * 2 / Lbox;
   wn_scale_kernel<<<(unsigned) ((size_t) Ng * Ng), IC_NT, 0, m->stream>>>(
       m->spec[0], pk->d_tab, pk->n, pk->log ? 1 : 0, Ng, m->Nk, m->Nkp, kfac,
-      log(kfac), pow(Lbox, -1.5));
+      log(kfac), pow(Lbox, -1.5)); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }

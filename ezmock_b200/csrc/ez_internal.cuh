@@ -81,6 +81,7 @@ struct EzMesh {
   cudaEvent_t ev[2 * ST_NSTAGE];
   bool ev_used[ST_NSTAGE];
   int timing;              // record per-stage events
+  cudaEvent_t mark[8];     // caller-placed events on the instance stream
   int cic_mode;            // 0: float atomics, 1: deterministic fixed-point
 
   int Ng;
@@ -100,6 +101,7 @@ struct EzMesh {
   unsigned long long *fixacc;   // deterministic CIC accumulators (4 x N)
   real *cat;               // device catalogue (6 x cap)
   size_t cat_cap;
+  size_t cat_n;            // length of the last catalogue (array stride)
   real *h_stage;           // pinned host staging for the catalogue
   size_t h_stage_cap;
 };
@@ -139,9 +141,14 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
     double vfac, const real *params, const size_t *pdf, int nmax,
     size_t ncell, size_t ntot, EzPopResult *res);
 
+// Counts kernel launches made by the library (reported to benchmarks).
+void ez_count_launch();
+
 // ---- memory ----
 int ez_mesh_alloc(EzMesh *m, int Ng);
 int ez_scratch(EzMesh *m, size_t bytes);
 int ez_rng_scratch(EzMesh *m, size_t bytes);
+int ez_select_counts(EzMesh *m, const unsigned long long *h, size_t *pdf,
+    int nmax, size_t *ncell, size_t *ntot, int16_t *d_nt);
 void ez_stage_begin(EzMesh *m, int st);
 void ez_stage_end(EzMesh *m, int st);

@@ -313,6 +313,19 @@ tracer_count_kernel(const real *__restrict__ rhot, size_t N,
 }
 
 __global__ void __launch_bounds__(NT)
+nt_kernel(const real *__restrict__ rhot, size_t N,
+    const BoundOut *__restrict__ bo, int16_t *nt) {
+  __shared__ real slo[EZ_MAX_NT];
+  __shared__ int sntr[EZ_MAX_NT];
+  const int nb = bo->nbins;
+  for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
+  __syncthreads();
+  for (size_t id = (size_t) blockIdx.x * blockDim.x + threadIdx.x; id < N;
+       id += (size_t) gridDim.x * blockDim.x)
+    nt[id] = (int16_t) cell_count(rhot[id], slo, sntr, nb);
+}
+
+__global__ void __launch_bounds__(NT)
 emit_kernel(const real *__restrict__ rhot, size_t N, int Ng,
     const BoundOut *__restrict__ bo, const unsigned long long *__restrict__ off,
     const uint32_t *__restrict__ draws, int ran, real gs, double Lbox,
@@ -453,7 +466,114 @@ int ensure_draws(EzMesh *m, size_t count) {
   return 0;
 }
 
+
+struct PopScratch {
+  unsigned long long *bcnt, *bscan, *hist, *dpdf, *dcount, *dcscan, *counter;
+  BoundOut *bo;
+};
+
+int pop_scratch(EzMesh *m, PopScratch *ps) {
+  const size_t N = m->N;
+  const size_t nblk = (N + CH - 1) / CH;
+  const size_t ntile_max = (N + TILE - 1) / TILE;
+  const size_t off_cnt = 0;
+  const size_t off_scan = off_cnt + (nblk + 1) * 8;
+  const size_t off_hist = off_scan + (nblk + 1) * 8;
+  const size_t off_bo = (off_hist + EZ_NLOGB * 8 + 255) / 256 * 256;
+  const size_t off_pdf = (off_bo + sizeof(BoundOut) + 255) / 256 * 256;
+  const size_t off_dc = (off_pdf + EZ_MAX_NT * 8 + 255) / 256 * 256;
+  const size_t off_dcs = off_dc + (256 * ntile_max + 1) * 8;
+  const size_t off_ctr = off_dcs + (256 * ntile_max + 1) * 8;
+  int e = ez_scratch(m, off_ctr + 64);
+  if (e) return e;
+  char *sc = (char *) m->scratch;
+  ps->bcnt = (unsigned long long *) (sc + off_cnt);
+  ps->bscan = (unsigned long long *) (sc + off_scan);
+  ps->hist = (unsigned long long *) (sc + off_hist);
+  ps->bo = (BoundOut *) (sc + off_bo);
+  ps->dpdf = (unsigned long long *) (sc + off_pdf);
+  ps->dcount = (unsigned long long *) (sc + off_dc);
+  ps->dcscan = (unsigned long long *) (sc + off_dcs);
+  ps->counter = (unsigned long long *) (sc + off_ctr);
+  return 0;
+}
+
+struct HostBounds {
+  unsigned long long ncell, ntot;
+  int err;
+  int nbins;
+};
+
+// Selection (pop_tracer.c:359-461): cut from the log2 histogram, compaction
+// of the candidates, radix sort of their keys, PDF-bin boundaries with the
+// tie extension.  Leaves the boundaries in ps.bo on the device.
+int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
+    const unsigned long long *h, const size_t *pdf, int nmax, size_t ncell,
+    size_t ntot, HostBounds *hb) {
+  const size_t N = m->N;
+  cudaStream_t st = m->stream;
+  skey_t *keys_a = (skey_t *) m->spec[1];
+  skey_t *keys_b = (skey_t *) m->spec[2];
+  int imax;
+  size_t cnt = 0;
+  for (imax = 0; imax < EZ_NLOGB; imax++) {
+    cnt += h[imax];
+    if (cnt >= ncell) break;
+  }
+  const real ilogb_max = 5;
+  const real cut = (imax == EZ_NLOGB - 1) ? (real) EZ_REAL_MIN
+      : (real) pow(2.0, (double) ilogb_max - imax);
+  cudaMemsetAsync(ps.counter, 0, 8, st);
+  compact_kernel<<<grid_for(N, NT), NT, 0, st>>>(rhot, N, cut, keys_a, ps.counter); ez_count_launch();
+  unsigned long long M = 0;
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(&M, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+    return EZMOCK_ERR_UNKNOWN;
+  skey_t *sorted = keys_a;
+  if (M > 1) {
+    const size_t ntiles = (M + TILE - 1) / TILE;
+    skey_t *src = keys_a, *dst = keys_b;
+    for (int shift = 0; shift < (int) (8 * sizeof(skey_t)); shift += 8) {
+      digit_hist_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, M, shift, ps.dcount, ntiles); ez_count_launch();
+      scan_kernel<<<1, 1024, 0, st>>>(ps.dcount, ps.dcscan, 256 * ntiles); ez_count_launch();
+      digit_scatter_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, dst, M, shift, ps.dcscan, ntiles); ez_count_launch();
+      skey_t *t = src; src = dst; dst = t;
+    }
+    sorted = src;
+  }
+  std::vector<unsigned long long> hp(nmax);
+  for (int j = 0; j < nmax; j++) hp[j] = pdf[j];
+  cudaMemcpyAsync(ps.dpdf, hp.data(), nmax * 8, cudaMemcpyHostToDevice, st);
+  bounds_kernel<<<1, 1, 0, st>>>(sorted, M, ps.dpdf, nmax, ncell, ntot, ps.bo); ez_count_launch();
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(hb, ps.bo, sizeof(*hb), cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+    return EZMOCK_ERR_UNKNOWN;
+  return 0;
+}
+
 }  // namespace
+
+// Selection on a tracer-density field already in spec[0] (test entry):
+// per-cell counts into nt (device), updated pdf/ncell/ntot.
+int ez_select_counts(EzMesh *m, const unsigned long long *h, size_t *pdf,
+    int nmax, size_t *ncell, size_t *ntot, int16_t *d_nt) {
+  PopScratch ps;
+  int e = pop_scratch(m, &ps);
+  if (e) return e;
+  HostBounds hb;
+  const real *rhot = (const real *) m->spec[0];
+  if ((e = select_stage(m, ps, rhot, h, pdf, nmax, *ncell, *ntot, &hb))) return e;
+  if (hb.err) return hb.err;
+  nt_kernel<<<grid_for(m->N, NT), NT, 0, m->stream>>>(rhot, m->N, ps.bo, d_nt); ez_count_launch();
+  std::vector<unsigned long long> po(nmax);
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(po.data(), ps.bo->pdf, nmax * 8, cudaMemcpyDeviceToHost, m->stream)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
+    return EZMOCK_ERR_UNKNOWN;
+  for (int j = 0; j < nmax; j++) pdf[j] = po[j];
+  *ncell = hb.ncell;
+  *ntot = hb.ntot;
+  return 0;
+}
 
 int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
     double vfac, const real *params, const size_t *pdf, int nmax,
@@ -466,37 +586,17 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   int e;
   res->err = 0;
 
-  // scratch: block counts (nblk+1) x2, hist 64, bounds struct, pdf copy,
-  // sort digit counts (256 x tiles + 1)
-  const size_t ntile_max = (N + TILE - 1) / TILE;
-  const size_t off_cnt = 0;
-  const size_t off_scan = off_cnt + (nblk + 1) * 8;
-  const size_t off_hist = off_scan + (nblk + 1) * 8;
-  const size_t off_bo = (off_hist + EZ_NLOGB * 8 + 255) / 256 * 256;
-  const size_t off_pdf = (off_bo + sizeof(BoundOut) + 255) / 256 * 256;
-  const size_t off_dc = (off_pdf + EZ_MAX_NT * 8 + 255) / 256 * 256;
-  const size_t off_dcs = off_dc + (256 * ntile_max + 1) * 8;
-  const size_t off_ctr = off_dcs + (256 * ntile_max + 1) * 8;
-  if ((e = ez_scratch(m, off_ctr + 64))) return e;
-  char *sc = (char *) m->scratch;
-  unsigned long long *bcnt = (unsigned long long *) (sc + off_cnt);
-  unsigned long long *bscan = (unsigned long long *) (sc + off_scan);
-  unsigned long long *hist = (unsigned long long *) (sc + off_hist);
-  BoundOut *bo = (BoundOut *) (sc + off_bo);
-  unsigned long long *dpdf = (unsigned long long *) (sc + off_pdf);
-  unsigned long long *dcount = (unsigned long long *) (sc + off_dc);
-  unsigned long long *dcscan = (unsigned long long *) (sc + off_dcs);
-  unsigned long long *counter = (unsigned long long *) (sc + off_ctr);
-
+  PopScratch ps;
+  if ((e = pop_scratch(m, &ps))) return e;
+  unsigned long long *bcnt = ps.bcnt, *bscan = ps.bscan, *hist = ps.hist;
+  BoundOut *bo = ps.bo;
   real *rhot = (real *) m->spec[0];
-  skey_t *keys_a = (skey_t *) m->spec[1];
-  skey_t *keys_b = (skey_t *) m->spec[2];
   cudaStream_t st = m->stream;
 
   // ---- 1. valid ranks ----
   ez_stage_begin(m, ST_BIAS);
-  valid_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, N, thres, bcnt);
-  scan_kernel<<<1, 1024, 0, st>>>(bcnt, bscan, nblk);
+  valid_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, N, thres, bcnt); ez_count_launch();
+  scan_kernel<<<1, 1024, 0, st>>>(bcnt, bscan, nblk); ez_count_launch();
   unsigned long long nvalid = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(&nvalid, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
@@ -510,7 +610,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N << 1, nd_bias, m->draws))) return e;
   cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
   bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
-      (double) (real) EZ_GAUSS_WIDTH, bscan, m->draws, ran, hist);
+      (double) (real) EZ_GAUSS_WIDTH, bscan, m->draws, ran, hist); ez_count_launch();
   unsigned long long h[EZ_NLOGB];
   if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
@@ -519,41 +619,8 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
 
   // ---- 3. selection ----
   ez_stage_begin(m, ST_SELECT);
-  int imax;
-  size_t cnt = 0;
-  for (imax = 0; imax < EZ_NLOGB; imax++) {
-    cnt += h[imax];
-    if (cnt >= ncell) break;
-  }
-  const real ilogb_max = 5;
-  const real cut = (imax == EZ_NLOGB - 1) ? (real) EZ_REAL_MIN
-      : (real) pow(2.0, (double) ilogb_max - imax);
-  cudaMemsetAsync(counter, 0, 8, st);
-  compact_kernel<<<grid_for(N, NT), NT, 0, st>>>(rhot, N, cut, keys_a, counter);
-  unsigned long long M = 0;
-  if (!EZ_CUDA_OK(cudaMemcpyAsync(&M, counter, 8, cudaMemcpyDeviceToHost, st)) ||
-      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
-    return EZMOCK_ERR_UNKNOWN;
-  skey_t *sorted = keys_a;
-  if (M > 1) {
-    const size_t ntiles = (M + TILE - 1) / TILE;
-    skey_t *src = keys_a, *dst = keys_b;
-    for (int shift = 0; shift < (int) (8 * sizeof(skey_t)); shift += 8) {
-      digit_hist_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, M, shift, dcount, ntiles);
-      scan_kernel<<<1, 1024, 0, st>>>(dcount, dcscan, 256 * ntiles);
-      digit_scatter_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, dst, M, shift, dcscan, ntiles);
-      skey_t *t = src; src = dst; dst = t;
-    }
-    sorted = src;
-  }
-  std::vector<unsigned long long> hp(nmax);
-  for (int j = 0; j < nmax; j++) hp[j] = pdf[j];
-  cudaMemcpyAsync(dpdf, hp.data(), nmax * 8, cudaMemcpyHostToDevice, st);
-  bounds_kernel<<<1, 1, 0, st>>>(sorted, M, dpdf, nmax, ncell, ntot, bo);
-  struct { unsigned long long ncell, ntot; int err; int nbins; } hb;
-  if (!EZ_CUDA_OK(cudaMemcpyAsync(&hb, bo, sizeof(hb), cudaMemcpyDeviceToHost, st)) ||
-      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
-    return EZMOCK_ERR_UNKNOWN;
+  HostBounds hb;
+  if ((e = select_stage(m, ps, rhot, h, pdf, nmax, ncell, ntot, &hb))) return e;
   ez_stage_end(m, ST_SELECT);
   if (hb.err) { res->err = hb.err; return 0; }
   res->ncell = hb.ncell;
@@ -569,10 +636,11 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
     if (!EZ_CUDA_OK(cudaMalloc(&m->cat, 6 * nt_all * sizeof(real)))) return EZMOCK_ERR_MEMORY;
     m->cat_cap = nt_all;
   }
+  m->cat_n = nt_all;
   real *cx = m->cat, *cy = cx + nt_all, *cz = cy + nt_all;
   real *cvx = cz + nt_all, *cvy = cvx + nt_all, *cvz = cvy + nt_all;
-  tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt);
-  scan_kernel<<<1, 1024, 0, st>>>(bcnt, bscan, nblk);
+  tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt); ez_count_launch();
+  scan_kernel<<<1, 1024, 0, st>>>(bcnt, bscan, nblk); ez_count_launch();
   unsigned long long ncount = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(&ncount, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
@@ -583,19 +651,19 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N * 5, 3 * nt_all, m->draws))) return e;
   const real gs = Lbox / Ng;
   emit_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, Ng, bo, bscan, m->draws,
-      ran, gs, Lbox, (unsigned long long) nt_all, cx, cy, cz);
+      ran, gs, Lbox, (unsigned long long) nt_all, cx, cy, cz); ez_count_launch();
   ez_stage_end(m, ST_EMIT);
 
   // ---- 5./6. velocities and dispersion ----
   ez_stage_begin(m, ST_VEL);
   const real igs = Ng / Lbox;
   vel_kernel<<<grid_for(nt_all, NT), NT, 0, st>>>(m->rho, m->paint[0],
-      m->paint[1], m->paint[2], Ng, igs, vfac, nt_all, cx, cy, cz, cvx, cvy, cvz);
+      m->paint[1], m->paint[2], Ng, igs, vfac, nt_all, cx, cy, cz, cvx, cvy, cvz); ez_count_launch();
   const size_t nd_disp = 6 * ((nt_all + 1) / 2);
   if ((e = ensure_draws(m, std::max(nd_disp, (size_t) 1)))) return e;
   if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N << 3, nd_disp, m->draws))) return e;
   disp_kernel<<<grid_for((nt_all + 1) / 2, NT), NT, 0, st>>>(nt_all, m->draws,
-      ran, (double) sigma_v, cvx, cvy, cvz);
+      ran, (double) sigma_v, cvx, cvy, cvz); ez_count_launch();
   ez_stage_end(m, ST_VEL);
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }

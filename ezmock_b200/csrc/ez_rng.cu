@@ -194,7 +194,7 @@ int mrg_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
   if (!nblk) return 0;
   mrg_fill_kernel<<<(unsigned) nblk, MRG_THREADS, 0, m->stream>>>(
       (uint32_t) s1[0], (uint32_t) s1[1], (uint32_t) s1[2], (uint32_t) s2[0],
-      (uint32_t) s2[1], (uint32_t) s2[2], start, count, g_mrg_thread_jump, out);
+      (uint32_t) s2[1], (uint32_t) s2[2], start, count, g_mrg_thread_jump, out); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
@@ -484,18 +484,20 @@ int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
   const size_t smem = (HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t);
   const int nbase = (int) plist.size() - p;
   // chunk 0 (state index 1) = jump of the seed window to `start`
-  if (nbase > 0)
+  if (nbase > 0) {
     mt_horner_kernel<<<1, H_THREADS, smem, m->stream>>>(states, states, 0, 1,
-        g_mt_xpow_dev, d_plist, nbase);
-  else
+        g_mt_xpow_dev, d_plist, nbase); ez_count_launch();
+  }
+  else {
     cudaMemcpyAsync(states + MT_N, states, MT_N * 4, cudaMemcpyDeviceToDevice, m->stream);
+  }
   for (int lev = 0; lev < p; lev++) {
     const unsigned nb = 1u << lev;
     mt_horner_kernel<<<nb, H_THREADS, smem, m->stream>>>(states, states, 1,
-        1 + nb, g_mt_xpow_dev, d_plist + nbase + lev, 1);
+        1 + nb, g_mt_xpow_dev, d_plist + nbase + lev, 1); ez_count_launch();
   }
   mt_gen_kernel<<<(unsigned) P, G_THREADS, 0, m->stream>>>(states + MT_N, L,
-      count, out);
+      count, out); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 

@@ -19,6 +19,7 @@ extern "C" {
 #define EZMOCKB200_OPT_CIC_MODE 1   /* 0: float atomics (default), 1: deterministic */
 #define EZMOCKB200_OPT_TIMING   2   /* 1: record per-stage CUDA-event timings */
 #define EZMOCKB200_OPT_DEVICE   3   /* CUDA device ordinal (before the first field) */
+#define EZMOCKB200_OPT_SEED     4   /* new random seed (> 0) for the next field */
 
 int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     int *err);
@@ -41,6 +42,16 @@ int EZmockB200_populate_device(EZMOCK *ez, const real *params,
 int EZmockB200_copy_catalog(EZMOCK *ez, real *x, real *y, real *z, real *vx,
     real *vy, real *vz, const size_t n, int *err);
 
+/* The GPU selection of cells (PDF bins with the tie extension,
+   libEZmock/EZmock/pop_tracer.c:359-509) applied to a given tracer-density
+   field `rhot` (Ngrid^3 host values) with its log2 histogram `hist` (64
+   counts) and PDF `pdf` (nmax counts, updated in place with the tie
+   extension, as are *ncell and *ntot).  Writes the number of tracers of every
+   cell to `nt` (Ngrid^3 values).  Needs a density field created first. */
+int EZmockB200_select_counts(EZMOCK *ez, const real *rhot,
+    const size_t *hist, size_t *pdf, const int nmax, size_t *ncell,
+    size_t *ntot, int16_t *nt, int *err);
+
 /* Raw 32-bit draws [start, start+count) of stream `seed` generated on the
    GPU (0: MRG32k3a, 1: MT19937). */
 int EZmockB200_rng_raw(const int randgen, const uint64_t seed,
@@ -51,6 +62,14 @@ int EZmockB200_sync(EZMOCK *ez);
 
 /* Size in bytes of `real` in this build (4 or 8). */
 int EZmockB200_real_size(void);
+
+/* Number of GPU kernels launched by the library in this process. */
+long long EZmockB200_launch_count(void);
+
+/* Records CUDA event `slot` (0..7) on the instance stream, and the device
+   time between two recorded slots (waits for the later one). */
+int EZmockB200_mark(EZMOCK *ez, const int slot);
+int EZmockB200_elapsed(EZMOCK *ez, const int a, const int b, double *ms);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,331 @@
+"""GPU parity: the CUDA library, called through its C-ABI (ctypes), against
+the CPU oracle and the reference's golden vectors.
+
+Tolerances:
+  * random draws, per-cell tracer counts, tracer positions: bit-exact;
+  * FP64 fields (psi, rho): max|gpu - oracle| <= 1e-12 * max|oracle|;
+  * FP64 velocities: <= 1e-9 * max|v| (atomic summation order of the
+    painted displacement grids);
+  * FP32 fields against the FP64 oracle: <= 5e-6 * max|oracle| (stated
+    field error of the production mode).
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from ezmock_b200 import EZmock, _lib
+from ezmock_b200.workloads import wiggle_pk
+from oracle.pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+PARAMS = [0.6, 15.0, 0.35, 300.0]
+
+
+def relmax(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def make(prec, Ng, L, rng, seed, k, P, Pnw=None, mBAO=0.0, logint=False):
+    m = EZmock(Lbox=L, Ngrid=Ng, rng=rng, seed=seed, prec=prec)
+    m.eval_growth_params(0.8, 0.31)
+    m.setup_linear_pk(k, P, Pnw, mBAO, logint)
+    return m
+
+
+def oracle_field(prec, Ng, L, rng, seed, k, P, fixamp=False, iphase=False, Pnw=None,
+                 mBAO=0.0, logint=False):
+    O = Oracle(prec)
+    g2, vf = O.growth(0.8, 0.0, 0.31)
+    t = O.pk_setup(Ng, L, g2, k, P, Pnw, mBAO, logint)
+    psi, rho = O.dens_field(t, Ng, L, rng, seed, fixamp, iphase)
+    return O, t, vf, psi, rho
+
+
+def cell_counts(x, y, z, Ng, L):
+    gs = L / Ng
+    idx = [np.floor(np.asarray(a, np.float64) / gs + 0.5).astype(np.int64) % Ng for a in (x, y, z)]
+    flat = (idx[0] * Ng + idx[1]) * Ng + idx[2]
+    return np.bincount(flat, minlength=Ng ** 3)
+
+
+@pytest.mark.parametrize("rng", [0, 1])
+@pytest.mark.parametrize("start,count", [(0, 2000), (12345, 70000), ((1 << 28) + 777, 5000),
+                                         (8 * 512 ** 3 + 3, 3000), (5 * 64 ** 3, 400000)])
+def test_rng_streams(rng, start, count):
+    L = _lib.load(64)
+    out = np.zeros(count, np.uint32)
+    assert L.EZmockB200_rng_raw(rng, 7, start, count, out.ctypes.data_as(ctypes.c_void_p)) == 0
+    assert np.array_equal(out, Oracle(64).rng_raw(rng, 7, start, count))
+
+
+@pytest.mark.parametrize("rng", [0, 1])
+@pytest.mark.parametrize("fixamp,iphase", [(False, False), (True, False), (False, True)])
+@pytest.mark.parametrize("Ng,L", [(32, 250.0), (40, 320.0), (24, 400.0)])
+def test_dens_field_fp64(pk_table, rng, fixamp, iphase, Ng, L):
+    k, P = pk_table
+    m = make(64, Ng, L, rng, 5, k, P)
+    m.create_dens_field_from_ic(fixamp=fixamp, iphase=iphase)
+    O, t, vf, psi, rho = oracle_field(64, Ng, L, rng, 5, k, P, fixamp, iphase)
+    for d in range(3):
+        assert relmax(m.field(d), psi[d]) <= TOL64
+    assert relmax(m.field(3), rho) <= TOL64
+
+
+@pytest.mark.parametrize("logint", [False, True])
+def test_dens_field_bao_logint_fp64(pk_table, logint):
+    k, Pnw = pk_table
+    P = wiggle_pk(k, Pnw)
+    m = make(64, 32, 250.0, 1, 9, k, P, Pnw, 3.0, logint)
+    m.create_dens_field_from_ic()
+    O, t, vf, psi, rho = oracle_field(64, 32, 250.0, 1, 9, k, P, Pnw=Pnw, mBAO=3.0, logint=logint)
+    assert relmax(m.field(3), rho) <= TOL64
+    assert relmax(m.field(0), psi[0]) <= TOL64
+
+
+def test_dens_field_fp32_error(pk_table):
+    k, P = pk_table
+    m = make(32, 64, 500.0, 1, 3, k, P)
+    m.create_dens_field_from_ic()
+    O, t, vf, psi, rho = oracle_field(64, 64, 500.0, 1, 3, k, P)
+    for d in range(3):
+        assert relmax(m.field(d), psi[d]) <= 5e-6
+    assert relmax(m.field(3), rho) <= 5e-6
+
+
+@pytest.mark.parametrize("rng", [0, 1])
+def test_golden_reference_fp64(golden, pk_table, rng):
+    """16^3 fields, counts and catalogue of the reference's own build."""
+    k, P = pk_table
+    tag = f"f64_rng{rng}_fa0"
+    m = make(64, 16, 200.0, rng, 7, k, P)
+    m.create_dens_field_from_ic()
+    psi = golden[tag + "_psi"]
+    for d in range(3):
+        assert relmax(m.field(d), psi[d]) <= TOL64
+    assert relmax(m.field(3), golden[tag + "_rho"]) <= TOL64
+    nexp = int(round(3e-4 * 200.0 ** 3))
+    cat = m.populate_tracer(*PARAMS, nexp)
+    ref = golden[tag + "_cat"]
+    assert len(cat[0]) == ref.shape[1]
+    for a in range(3):
+        assert np.array_equal(cat[a], ref[a])
+    vmax = np.abs(ref[3:]).max()
+    for a in range(3, 6):
+        assert np.abs(cat[a] - ref[a]).max() <= 1e-9 * vmax
+    assert np.array_equal(cell_counts(*cat[:3], 16, 200.0),
+                          golden[tag + "_nt"].reshape(-1).astype(np.int64))
+
+
+@pytest.mark.parametrize("rng", [0, 1])
+@pytest.mark.parametrize("params,n", [([0.6, 15.0, 0.35, 300.0], 3e-4),
+                                      ([1.2, 5.0, 0.2, 150.0], 1e-4),
+                                      ([0.3, 30.0, 0.6, 500.0], 5e-4),
+                                      ([0.0, 10.0, 0.3, 0.0], 2e-4)])
+def test_populate_fp64(pk_table, rng, params, n):
+    k, P = pk_table
+    Ng, L = 48, 400.0
+    m = make(64, Ng, L, rng, 2, k, P)
+    m.create_dens_field_from_ic()
+    nexp = int(n * L ** 3)
+    cat = m.populate_tracer(*params, nexp)
+    O, t, vf, psi, rho = oracle_field(64, Ng, L, rng, 2, k, P)
+    e, ref = O.populate(Ng, L, rng, 2, vf, psi, rho, params, nexp)
+    assert e == 0
+    assert len(cat[0]) == len(ref[0])
+    assert np.array_equal(cell_counts(*cat[:3], Ng, L), cell_counts(*ref[:3], Ng, L))
+    for a in range(3):
+        assert np.array_equal(cat[a], ref[a])
+    vmax = np.abs(np.stack(ref[3:])).max()
+    for a in range(3, 6):
+        assert np.abs(cat[a] - ref[a]).max() <= 1e-9 * vmax
+
+
+def test_populate_fp32_positions(pk_table):
+    """FP32: on the GPU's own density field the oracle reproduces the
+    catalogue positions bit for bit."""
+    k, P = pk_table
+    Ng, L = 64, 500.0
+    m = make(32, Ng, L, 1, 4, k, P)
+    m.create_dens_field_from_ic()
+    nexp = int(3e-4 * L ** 3)
+    cat = m.populate_tracer(*PARAMS, nexp)
+    O = Oracle(32)
+    _, vf = O.growth(0.8, 0.0, 0.31)
+    e, ref = O.populate(Ng, L, 1, 4, vf, [m.field(d) for d in range(3)], m.field(3), PARAMS, nexp)
+    assert e == 0 and len(ref[0]) == len(cat[0])
+    for a in range(3):
+        assert np.array_equal(cat[a], ref[a])
+    vmax = np.abs(np.stack(ref[3:])).max()
+    for a in range(3, 6):
+        assert np.abs(cat[a] - ref[a]).max() <= 1e-4 * vmax
+
+
+def test_repeated_populations_fp64(pk_table):
+    """Several populations on one density field (the field is not modified)."""
+    k, P = pk_table
+    Ng, L = 32, 250.0
+    m = make(64, Ng, L, 0, 11, k, P)
+    m.create_dens_field_from_ic()
+    O, t, vf, psi, rho = oracle_field(64, Ng, L, 0, 11, k, P)
+    for params, n in [([0.5, 10.0, 0.3, 250.0], 2e-4), ([0.9, 20.0, 0.4, 350.0], 1e-4),
+                      ([1.3, 30.0, 0.5, 450.0], 2e-5 * 10)]:
+        nexp = int(n * L ** 3)
+        cat = m.populate_tracer(*params, nexp)
+        e, ref = O.populate(Ng, L, 0, 11, vf, psi, rho, params, nexp)
+        assert e == 0 and len(cat[0]) == len(ref[0])
+        for a in range(3):
+            assert np.array_equal(cat[a], ref[a])
+
+
+def test_white_noise_fp64(pk_table):
+    k, P = pk_table
+    Ng, L = 32, 250.0
+    delta = np.random.default_rng(8).standard_normal(Ng ** 3)
+    m = make(64, Ng, L, 1, 1, k, P)
+    m.create_dens_field_from_wn(delta)
+    O = Oracle(64)
+    g2, vf = O.growth(0.8, 0.0, 0.31)
+    t = O.pk_setup(Ng, L, g2, k, P)
+    psi = O.disp_whitenoise(t, Ng, L, delta)
+    for d in range(3):
+        assert relmax(m.field(d), psi[d]) <= TOL64
+    assert relmax(m.field(3), O.cic(Ng, L, psi)) <= TOL64
+
+
+@pytest.mark.parametrize("deepcopy", [False, True])
+def test_user_displacements_fp64(pk_table, deepcopy):
+    k, P = pk_table
+    Ng, L = 32, 250.0
+    O, t, vf, psi, rho = oracle_field(64, Ng, L, 1, 6, k, P)
+    m = make(64, Ng, L, 1, 6, k, P)
+    m.create_dens_field_from_disp(*[p.reshape(-1) for p in psi], deepcopy=deepcopy)
+    assert relmax(m.field(3), rho) <= TOL64
+    nexp = int(3e-4 * L ** 3)
+    cat = m.populate_tracer(*PARAMS, nexp)
+    e, ref = O.populate(Ng, L, 1, 6, vf, psi, rho, PARAMS, nexp)
+    assert e == 0 and len(cat[0]) == len(ref[0])
+    for a in range(3):
+        assert np.array_equal(cat[a], ref[a])
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+def test_deterministic_cic(pk_table, prec):
+    k, P = pk_table
+    Ng, L = 48, 400.0
+    m = make(prec, Ng, L, 1, 2, k, P)
+    m.set_option(1, 1)
+    m.create_dens_field_from_ic()
+    r1 = m.field(3).copy()
+    q1 = m.field(4).copy()
+    m.create_dens_field_from_ic()
+    assert np.array_equal(r1, m.field(3)) and np.array_equal(q1, m.field(4))
+    O, t, vf, psi, rho = oracle_field(64, Ng, L, 1, 2, k, P)
+    assert relmax(r1, rho) <= (TOL64 if prec == 64 else 5e-6)
+
+
+def _select(m, prec, rhot, hist, pdf, nmax, ncell, ntot):
+    L = m._L
+    rdt = np.float32 if prec == 32 else np.float64
+    rhot = np.ascontiguousarray(rhot, rdt).reshape(-1)
+    hist = np.ascontiguousarray(hist, np.uintp)
+    pdf = np.array(pdf, np.uintp)
+    nc, no = ctypes.c_size_t(ncell), ctypes.c_size_t(ntot)
+    nt = np.zeros(rhot.size, np.int16)
+    err = ctypes.c_int(0)
+    r = L.EZmockB200_select_counts(m._ez, rhot.ctypes.data, hist.ctypes.data, pdf.ctypes.data,
+                                   nmax, ctypes.byref(nc), ctypes.byref(no), nt.ctypes.data,
+                                   ctypes.byref(err))
+    return r, nt, pdf, nc.value, no.value
+
+
+def test_selection_ties_golden(golden, pk_table):
+    k, P = pk_table
+    m = make(64, 16, 200.0, 1, 3, k, P)
+    m.create_dens_field_from_ic()
+    nmax, ncell, ntot = (int(v) for v in golden["ties_in"])
+    r, nt, pdf, nc, no = _select(m, 64, golden["ties_rhot"], golden["ties_hist"],
+                                 golden["ties_pdf_in"], nmax, ncell, ntot)
+    assert r == 0
+    assert np.array_equal(nt.reshape(16, 16, 16), golden["ties_nt"])
+    assert list(pdf) == list(golden["ties_pdf_out"])
+    assert [nc, no] == list(golden["ties_out"])
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+def test_selection_ties_random(pk_table, prec):
+    k, P = pk_table
+    Ng = 32
+    m = make(prec, Ng, 250.0, 1, 3, k, P)
+    m.create_dens_field_from_ic()
+    O = Oracle(prec)
+    rs = np.random.default_rng(5)
+    done = 0
+    for trial in range(10):
+        nv = int(rs.choice([300, 3000, 30000]))
+        vals = np.exp(rs.uniform(-3, 3.5, nv)).astype(O.rdt)
+        rhot = vals[rs.integers(0, nv, Ng ** 3)]
+        rhot[rs.random(Ng ** 3) < 0.3] = 0
+        lb = np.floor(np.log2(rhot[rhot > 0].astype(np.float64))).astype(int)
+        hist = np.zeros(64, np.uintp)
+        np.add.at(hist, np.clip(5 - lb, 0, 63), 1)
+        e, pdf, nmax, ncell, ntot = O.eval_pdf(Ng, int(rs.integers(500, 8000)),
+                                               float(rs.uniform(0.2, 0.6)))
+        if e or ncell > (rhot > 0).sum():
+            continue
+        e2, nt_o, pdf_o, nc_o, no_o = O.select(Ng, rhot.reshape(Ng, Ng, Ng), hist, pdf,
+                                               nmax, ncell, ntot)
+        r, nt, pdf_g, nc, no = _select(m, prec, rhot, hist, pdf, nmax, ncell, ntot)
+        assert r == e2
+        if r:
+            continue
+        assert np.array_equal(nt, nt_o.reshape(-1))
+        assert list(pdf_g) == list(pdf_o) and (nc, no) == (nc_o, no_o)
+        done += 1
+    assert done >= 3
+
+
+def test_write_ascii(pk_table, tmp_path):
+    k, P = pk_table
+    m = make(32, 32, 250.0, 1, 1, k, P)
+    m.create_dens_field_from_ic()
+    fn = tmp_path / "cat.txt"
+    m.populate_tracer_to_file(*PARAMS, int(3e-4 * 250.0 ** 3), str(fn), rsd_fac=0.0113)
+    lines = fn.read_text().splitlines()
+    assert lines[0].startswith("# BOX_SIZE=250 , NUM_GRID=32")
+    assert lines[3] == "# RAND_GENERATOR=MT19937 , RAND_SEED=1"
+    assert lines[4] == "# x(1) y(2) z_rsd(3)"
+    cat = m.populate_tracer(*PARAMS, int(3e-4 * 250.0 ** 3))
+    x, z, vz = cat[0][0], cat[2][0], cat[5][0]
+    zr = float(z) + 0.0113 * float(vz)
+    if zr >= 250.0:
+        zr -= 250.0
+    if zr < 0:
+        zr += 250.0
+    assert lines[5].split()[0] == "%.6g" % x
+    assert lines[5].split()[2] == "%.6g" % zr
+    assert len(lines) == 5 + len(cat[0])
+
+
+def test_error_paths(pk_table):
+    k, P = pk_table
+    m = make(64, 32, 250.0, 1, 1, k, P)
+    with pytest.raises(RuntimeError, match="density fields uninitialized"):
+        m.populate_tracer(*PARAMS, 4000)
+    m = make(64, 32, 250.0, 1, 1, k, P)
+    m.create_dens_field_from_ic()
+    with pytest.raises(RuntimeError, match="too many expected"):
+        m.populate_tracer(*PARAMS, 32 ** 3)
+    m = make(64, 32, 250.0, 1, 1, k, P)
+    m.create_dens_field_from_ic()
+    with pytest.raises(RuntimeError, match="invalid base number"):
+        m.populate_tracer(0.6, 15.0, 1.0, 300.0, 4000)
+    m = make(64, 32, 250.0, 1, 1, k, P)
+    m.create_dens_field_from_ic()
+    with pytest.raises(RuntimeError, match="not enough cells"):
+        m.populate_tracer(50.0, 15.0, 0.35, 300.0, 20000)
