@@ -87,6 +87,120 @@ cic_atomic_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
   }
 }
 
+#ifdef SINGLE_PREC
+// ---- slab kernel: shared-memory accumulation with a sliding z window ----
+//
+// A CTA owns the particles of a 16 x 16 column of Lagrangian cells and walks
+// it along z in chunks of 8 slices.  Contributions land in a shared-memory
+// ring of 16 z slices covering the column widened by H = 2 cells on each
+// side (plus the CIC neighbour), for rho and the three momenta.  After each
+// chunk the slices no later particle can reach are added to global memory
+// with 16-byte vector atomics (4 consecutive z cells) and cleared.  Particles
+// displaced by more than H cells fall back to direct global atomics.  Needs
+// Ng a multiple of 16.
+constexpr int ST = 16;                       // column tile (x and y)
+constexpr int SH = 2;                        // halo
+constexpr int SB = ST + 2 * SH + 1;          // box side = 21
+constexpr int SKZ = 8;                       // z slices per chunk
+constexpr int SRING = 16;                    // ring length (z slices)
+constexpr int SLAB_NT = 512;
+constexpr int SQ = SB * SB * SRING;          // floats per quantity
+
+__device__ __forceinline__ void gadd(real *g, real v) { atomicAdd(g, v); }
+
+__global__ void __launch_bounds__(SLAB_NT)
+cic_slab_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
+    const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
+    int Ng, real igs) {
+  extern __shared__ float ring[];            // [4][SB][SB][SRING]
+  const int ntile = Ng / ST;
+  const int i0 = (blockIdx.x / ntile) * ST, j0 = (blockIdx.x % ntile) * ST;
+  for (int e = threadIdx.x; e < 4 * SQ; e += SLAB_NT) ring[e] = 0;
+  __syncthreads();
+  int U = -4;                                // oldest unflushed z (multiple of 4)
+  const int nchunk = Ng / SKZ;
+  for (int c = 0; c <= nchunk; c++) {
+    if (c < nchunk) {
+      const int zc = c * SKZ;
+      for (int p = threadIdx.x; p < ST * ST * SKZ; p += SLAB_NT) {
+        const int kz = p & (SKZ - 1), tj = (p >> 3) & (ST - 1), ti = p >> 7;
+        const int i = i0 + ti, j = j0 + tj, k = zc + kz;
+        const size_t id = ((size_t) i * Ng + j) * Ng + k;
+        const real pv[3] = {p0[id], p1[id], p2[id]};
+        // positions and weights as in dens_field.c:262-289 (unwrapped cells)
+        const real x = pv[0] * igs + i, y = pv[1] * igs + j, z = pv[2] * igs + k;
+        const int x0 = (int) floor((double) x), y0 = (int) floor((double) y),
+                  z0 = (int) floor((double) z);
+        const real wx1 = x - x0, wx0 = 1 - wx1;
+        const real wy1 = y - y0, wy0 = 1 - wy1;
+        const real wz1 = z - z0, wz0 = 1 - wz1;
+        const int rx = x0 - (i0 - SH), ry = y0 - (j0 - SH);
+        const bool inbox = rx >= 0 && rx <= SB - 2 && ry >= 0 && ry <= SB - 2 &&
+            z0 >= zc - SH && z0 <= zc + SKZ - 1 + SH;
+        const real wxs[2] = {wx0, wx1}, wys[2] = {wy0, wy1}, wzs[2] = {wz0, wz1};
+        if (inbox) {
+#pragma unroll
+          for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+#pragma unroll
+              for (int cz = 0; cz < 2; cz++) {
+                const int base = ((rx + a) * SB + (ry + b)) * SRING + ((z0 + cz) & (SRING - 1));
+                const real w = wxs[a] * wys[b] * wzs[cz];
+                atomicAdd(ring + base, (float) w);
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+                  atomicAdd(ring + (d + 1) * SQ + base, (float) ((wxs[a] * pv[d]) * wys[b] * wzs[cz]));
+              }
+        }
+        else {
+          int xs[2], ys[2], zs[2];
+          xs[0] = ((x0 % Ng) + Ng) % Ng; xs[1] = (xs[0] == Ng - 1) ? 0 : xs[0] + 1;
+          ys[0] = ((y0 % Ng) + Ng) % Ng; ys[1] = (ys[0] == Ng - 1) ? 0 : ys[0] + 1;
+          zs[0] = ((z0 % Ng) + Ng) % Ng; zs[1] = (zs[0] == Ng - 1) ? 0 : zs[0] + 1;
+#pragma unroll
+          for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+#pragma unroll
+              for (int cz = 0; cz < 2; cz++) {
+                const size_t g = ((size_t) xs[a] * Ng + ys[b]) * Ng + zs[cz];
+                gadd(rho + g, wxs[a] * wys[b] * wzs[cz]);
+                gadd(q0 + g, (wxs[a] * pv[0]) * wys[b] * wzs[cz]);
+                gadd(q1 + g, (wxs[a] * pv[1]) * wys[b] * wzs[cz]);
+                gadd(q2 + g, (wxs[a] * pv[2]) * wys[b] * wzs[cz]);
+              }
+        }
+      }
+    }
+    __syncthreads();
+    // flush the quads of z slices no later particle can reach
+    const int zfinal = (c < nchunk) ? (c + 1) * SKZ - SH : Ng + SH + 2;
+    int nq = 0;
+    while (U + 4 * (nq + 1) <= zfinal) nq++;
+    const int ntask = nq * 4 * SB * SB;
+    for (int t = threadIdx.x; t < ntask; t += SLAB_NT) {
+      const int qd = t / (4 * SB * SB);
+      const int r = t - qd * 4 * SB * SB;
+      const int q = r / (SB * SB), col = r - q * SB * SB;
+      const int rx = col / SB, ry = col - rx * SB;
+      const int zq = U + 4 * qd;
+      float4 *src = (float4 *) (ring + q * SQ + col * SRING + (zq & (SRING - 1)));
+      const float4 v = *src;
+      *src = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+      const int gx = (((i0 - SH + rx) % Ng) + Ng) % Ng;
+      const int gy = (((j0 - SH + ry) % Ng) + Ng) % Ng;
+      const int gz = ((zq % Ng) + Ng) % Ng;
+      real *gq = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
+      atomicAdd((float4 *) (gq + ((size_t) gx * Ng + gy) * Ng + gz), v);
+    }
+    U += 4 * nq;
+    __syncthreads();
+  }
+}
+#endif
+
 // ---- deterministic mode: 64-bit fixed point ----
 constexpr double FIX_RHO = 1125899906842624.0;    // 2^50: rho < 8192 per cell
 constexpr double FIX_MOM = 1099511627776.0;       // 2^40: |sum psi w| < 2^23
@@ -167,8 +281,24 @@ int ez_cic(EzMesh *m, double Lbox) {
     for (int d = 0; d < 3; d++)
       if (!EZ_CUDA_OK(cudaMemsetAsync(m->paint[d], 0, N * sizeof(real), m->stream)))
         return EZMOCK_ERR_UNKNOWN;
-    cic_atomic_kernel<true><<<grid, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
-        m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, N); ez_count_launch();
+#ifdef SINGLE_PREC
+    if (Ng % ST == 0 && Ng >= 2 * ST) {
+      static bool attr = false;
+      const size_t smem = 4 * SQ * sizeof(float);
+      if (!attr) {
+        cudaFuncSetAttribute(cic_slab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        attr = true;
+      }
+      cic_slab_kernel<<<(unsigned) ((Ng / ST) * (Ng / ST)), SLAB_NT, smem, m->stream>>>(
+          m->psi[0], m->psi[1], m->psi[2], m->rho, m->paint[0], m->paint[1],
+          m->paint[2], Ng, igs); ez_count_launch();
+    }
+    else
+#endif
+    {
+      cic_atomic_kernel<true><<<grid, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
+          m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, N); ez_count_launch();
+    }
   }
   ez_stage_end(m, ST_CIC);
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;

@@ -140,22 +140,74 @@ bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
     atomicAdd(hist + threadIdx.x, (unsigned long long) sh[threadIdx.x]);
 }
 
+// Candidates (rho_t >= cut) of a 4096-cell chunk are counted, one atomic per
+// block reserves their slots, and their keys are written (the order of the
+// candidate list is irrelevant: it is sorted next).
 __global__ void __launch_bounds__(NT)
 compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
     skey_t *__restrict__ keys, unsigned long long *counter) {
-  for (size_t id = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
-       id - threadIdx.x < N; id += (size_t) gridDim.x * blockDim.x) {
-    bool take = false;
-    real v = 0;
-    if (id < N) { v = rhot[id]; take = !(v < thres); }
-    const unsigned mask = __ballot_sync(0xffffffffu, take);
-    if (!mask) continue;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(counter, (unsigned long long) __popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (take) keys[base + __popc(mask & ((1u << lane) - 1))] = to_key(v);
+  __shared__ unsigned long long sw[32];
+  __shared__ unsigned long long sbase;
+  const size_t b0 = (size_t) blockIdx.x * CH;
+  real v[ROWS];
+  unsigned int c = 0;
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    v[q] = (id < N) ? rhot[id] : (real) 0;
+    c += (id < N && !(v[q] < thres));
+  }
+  unsigned long long tot;
+  unsigned long long off = block_scan<unsigned long long>((unsigned long long) c, &tot, sw);
+  if (threadIdx.x == 0) sbase = tot ? atomicAdd(counter, tot) : 0;
+  __syncthreads();
+  off += sbase;
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    if (id < N && !(v[q] < thres)) keys[off++] = to_key(v[q]);
+  }
+}
+
+// Multi-block exclusive scan for long arrays: chunk sums, a scan of the sums,
+// then each chunk rescanned with its offset.  out[n] = total.
+constexpr int SCAN_CHUNK = 8192;
+
+__global__ void __launch_bounds__(1024)
+chunk_sum_kernel(const unsigned long long *__restrict__ in, size_t n,
+    unsigned long long *sums) {
+  __shared__ unsigned long long sw[32];
+  const size_t c0 = (size_t) blockIdx.x * SCAN_CHUNK;
+  unsigned long long s = 0;
+  for (int e = threadIdx.x; e < SCAN_CHUNK; e += 1024) {
+    const size_t g = c0 + e;
+    if (g < n) s += in[g];
+  }
+  unsigned long long tot;
+  block_scan<unsigned long long>(s, &tot, sw);
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024)
+chunk_scan_kernel(const unsigned long long *__restrict__ in, size_t n,
+    const unsigned long long *__restrict__ offs, unsigned long long *out) {
+  __shared__ unsigned long long sw[32];
+  const size_t c0 = (size_t) blockIdx.x * SCAN_CHUNK;
+  constexpr int PER = SCAN_CHUNK / 1024;
+  unsigned long long v[PER], loc = 0;
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    const size_t g = c0 + (size_t) threadIdx.x * PER + j;
+    v[j] = (g < n) ? in[g] : 0;
+    loc += v[j];
+  }
+  unsigned long long tot;
+  unsigned long long run = offs[blockIdx.x] + block_scan<unsigned long long>(loc, &tot, sw);
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    const size_t g = c0 + (size_t) threadIdx.x * PER + j;
+    if (g < n) out[g] = run;
+    run += v[j];
   }
 }
 
@@ -467,8 +519,23 @@ int ensure_draws(EzMesh *m, size_t count) {
 }
 
 
+// Exclusive scan of n values into out[0..n], out[n] = total.  `tmp` holds
+// ceil(n / SCAN_CHUNK) + 1 values.
+void scan_u64(const unsigned long long *in, unsigned long long *out, size_t n,
+    unsigned long long *tmp, cudaStream_t st) {
+  if (n <= 4 * SCAN_CHUNK) {
+    scan_kernel<<<1, 1024, 0, st>>>(in, out, n); ez_count_launch();
+    return;
+  }
+  const size_t nc = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+  chunk_sum_kernel<<<(unsigned) nc, 1024, 0, st>>>(in, n, tmp); ez_count_launch();
+  scan_kernel<<<1, 1024, 0, st>>>(tmp, tmp, nc); ez_count_launch();
+  chunk_scan_kernel<<<(unsigned) nc, 1024, 0, st>>>(in, n, tmp, out); ez_count_launch();
+  cudaMemcpyAsync(out + n, tmp + nc, 8, cudaMemcpyDeviceToDevice, st);
+}
+
 struct PopScratch {
-  unsigned long long *bcnt, *bscan, *hist, *dpdf, *dcount, *dcscan, *counter;
+  unsigned long long *bcnt, *bscan, *hist, *dpdf, *dcount, *dcscan, *counter, *tmp;
   BoundOut *bo;
 };
 
@@ -484,7 +551,9 @@ int pop_scratch(EzMesh *m, PopScratch *ps) {
   const size_t off_dc = (off_pdf + EZ_MAX_NT * 8 + 255) / 256 * 256;
   const size_t off_dcs = off_dc + (256 * ntile_max + 1) * 8;
   const size_t off_ctr = off_dcs + (256 * ntile_max + 1) * 8;
-  int e = ez_scratch(m, off_ctr + 64);
+  const size_t off_tmp = off_ctr + 64;
+  const size_t ntmp = (256 * ntile_max + nblk) / SCAN_CHUNK + 8;
+  int e = ez_scratch(m, off_tmp + ntmp * 8);
   if (e) return e;
   char *sc = (char *) m->scratch;
   ps->bcnt = (unsigned long long *) (sc + off_cnt);
@@ -495,6 +564,7 @@ int pop_scratch(EzMesh *m, PopScratch *ps) {
   ps->dcount = (unsigned long long *) (sc + off_dc);
   ps->dcscan = (unsigned long long *) (sc + off_dcs);
   ps->counter = (unsigned long long *) (sc + off_ctr);
+  ps->tmp = (unsigned long long *) (sc + off_tmp);
   return 0;
 }
 
@@ -524,7 +594,8 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
   const real cut = (imax == EZ_NLOGB - 1) ? (real) EZ_REAL_MIN
       : (real) pow(2.0, (double) ilogb_max - imax);
   cudaMemsetAsync(ps.counter, 0, 8, st);
-  compact_kernel<<<grid_for(N, NT), NT, 0, st>>>(rhot, N, cut, keys_a, ps.counter); ez_count_launch();
+  compact_kernel<<<(unsigned) ((N + CH - 1) / CH), NT, 0, st>>>(rhot, N, cut, keys_a,
+      ps.counter); ez_count_launch();
   unsigned long long M = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(&M, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
@@ -535,7 +606,7 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
     skey_t *src = keys_a, *dst = keys_b;
     for (int shift = 0; shift < (int) (8 * sizeof(skey_t)); shift += 8) {
       digit_hist_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, M, shift, ps.dcount, ntiles); ez_count_launch();
-      scan_kernel<<<1, 1024, 0, st>>>(ps.dcount, ps.dcscan, 256 * ntiles); ez_count_launch();
+      scan_u64(ps.dcount, ps.dcscan, 256 * ntiles, ps.tmp, st);
       digit_scatter_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, dst, M, shift, ps.dcscan, ntiles); ez_count_launch();
       skey_t *t = src; src = dst; dst = t;
     }
@@ -596,7 +667,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // ---- 1. valid ranks ----
   ez_stage_begin(m, ST_BIAS);
   valid_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, N, thres, bcnt); ez_count_launch();
-  scan_kernel<<<1, 1024, 0, st>>>(bcnt, bscan, nblk); ez_count_launch();
+  scan_u64(bcnt, bscan, nblk, ps.tmp, st);
   unsigned long long nvalid = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(&nvalid, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
@@ -640,7 +711,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   real *cx = m->cat, *cy = cx + nt_all, *cz = cy + nt_all;
   real *cvx = cz + nt_all, *cvy = cvx + nt_all, *cvz = cvy + nt_all;
   tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt); ez_count_launch();
-  scan_kernel<<<1, 1024, 0, st>>>(bcnt, bscan, nblk); ez_count_launch();
+  scan_u64(bcnt, bscan, nblk, ps.tmp, st);
   unsigned long long ncount = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(&ncount, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))

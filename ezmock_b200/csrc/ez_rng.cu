@@ -16,9 +16,9 @@
 //    at any offset J is p(T) applied to the seed window, p = x^J mod phi
 //    (Haramoto et al. 2008).  phi is found once on the host by
 //    Berlekamp-Massey and the table x^(2^k) mod phi by repeated squaring.  On
-//    the GPU one block applies p(T) with Horner's rule over 6-bit windows
-//    (a 64-entry table of combinations of T^j s held in shared memory, one
-//    barrier per window).  Chunk states for a range [start, start + P*L) are
+//    the GPU one block applies p(T) with Horner's rule over 16-bit windows
+//    (four 16-entry tables of combinations of T^j s held in shared memory,
+//    one barrier per window).  Chunk states for a range [start, start + P*L) are
 //    built by one jump to `start` followed by log2(P) doubling levels, each
 //    level jumping all known chunk states by 2^m * L in parallel.  Each chunk
 //    is then generated by one block with the three-phase twist.
@@ -204,8 +204,10 @@ int mrg_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
 
 constexpr int MT_N = 624, MT_M = 397, MT_DEG = 19937, MT_PW = 312;
 constexpr uint32_t MT_A = 0x9908b0dfU, MT_UP = 0x80000000U, MT_LO = 0x7fffffffU;
-constexpr int HW = 6;                                   // Horner window bits
-constexpr int HTAB = 1 << HW;
+constexpr int HW = 16;                                  // Horner window bits
+constexpr int HSUB = 4;                                 // bits per sub-table
+constexpr int HG = HW / HSUB;                           // sub-tables
+constexpr int HTAB = 1 << HSUB;                         // entries per sub-table
 constexpr int H_THREADS = 640;
 constexpr int G_THREADS = 640;
 
@@ -225,14 +227,17 @@ __device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
 
 // Apply p(T) for each polynomial in `plist` (npoly entries, each MT_PW words
 // in `polys`) to state in[in_base + blockIdx.x]; result to out[out_base + b].
-// States are 624-word windows in logical order.
+// States are 624-word windows in logical order.  Horner's rule runs over
+// 16-bit windows of p: r <- T^16 r + sum_g tab_g[c_g], where tab_g[c] =
+// sum_{j<4} c_j T^(4g+j) s are four 16-entry tables of combinations of the
+// source state (shared memory), so each window costs one barrier.
 __global__ void __launch_bounds__(H_THREADS)
 mt_horner_kernel(const uint32_t *__restrict__ states_in, uint32_t *states_out,
     size_t in_base, size_t out_base, const uint64_t *__restrict__ polys,
     const int *__restrict__ plist, int npoly) {
   extern __shared__ uint32_t sm[];
-  uint32_t *tab = sm;                        // HTAB x MT_N
-  uint32_t *ext = tab + HTAB * MT_N;         // MT_N + HW
+  uint32_t *tab = sm;                        // HG x HTAB x MT_N
+  uint32_t *ext = tab + HG * HTAB * MT_N;    // MT_N + HW
   uint32_t *ra = ext + MT_N + HW;            // MT_N
   uint32_t *rb = ra + MT_N;                  // MT_N
   const int t = threadIdx.x;
@@ -243,12 +248,13 @@ mt_horner_kernel(const uint32_t *__restrict__ states_in, uint32_t *states_out,
     const uint64_t *p = polys + (size_t) plist[ip] * MT_PW;
     if (t < HW) ext[MT_N + t] = mt_f(ext[t], ext[t + 1], ext[MT_M + t]);
     __syncthreads();
-    for (int e = t; e < HTAB * MT_N; e += blockDim.x) {
-      const int c = e / MT_N, k = e - c * MT_N;
+    for (int e = t; e < HG * HTAB * MT_N; e += blockDim.x) {
+      const int gc = e / MT_N, k = e - gc * MT_N;
+      const int g = gc / HTAB, c = gc - g * HTAB;
       uint32_t v = 0;
 #pragma unroll
-      for (int j = 0; j < HW; j++)
-        if (c & (1 << j)) v ^= ext[k + j];
+      for (int j = 0; j < HSUB; j++)
+        if (c & (1 << j)) v ^= ext[k + HSUB * g + j];
       tab[e] = v;
     }
     for (int k = t; k < MT_N; k += blockDim.x) ra[k] = 0;
@@ -256,11 +262,8 @@ mt_horner_kernel(const uint32_t *__restrict__ states_in, uint32_t *states_out,
     uint32_t *r0 = ra, *r1 = rb;
     const int nwin = (MT_DEG + HW - 1) / HW;
     for (int q = nwin - 1; q >= 0; q--) {
-      const int b = q * HW;
-      uint64_t bits = p[b >> 6] >> (b & 63);
-      if ((b & 63) + HW > 64 && (b >> 6) + 1 < MT_PW) bits |= p[(b >> 6) + 1] << (64 - (b & 63));
-      const int c = (int) (bits & (HTAB - 1));
-      const uint32_t *tc = tab + c * MT_N;
+      const int b = q * HW;                    // HW = 16 divides 64
+      const uint32_t bits = (uint32_t) (p[b >> 6] >> (b & 63)) & 0xffffu;
       if (t < MT_N) {
         uint32_t v;
         if (t < MT_N - HW) v = r0[t + HW];
@@ -268,7 +271,10 @@ mt_horner_kernel(const uint32_t *__restrict__ states_in, uint32_t *states_out,
           const int s = t - (MT_N - HW);
           v = mt_f(r0[s], r0[s + 1], r0[MT_M + s]);
         }
-        r1[t] = v ^ tc[t];
+#pragma unroll
+        for (int g = 0; g < HG; g++)
+          v ^= tab[(g * HTAB + ((bits >> (HSUB * g)) & (HTAB - 1))) * MT_N + t];
+        r1[t] = v;
       }
       __syncthreads();
       uint32_t *tmp = r0; r0 = r1; r1 = tmp;
@@ -448,7 +454,7 @@ int mt_prepare(int dev) {
     return EZMOCK_ERR_MEMORY;
   if (!EZ_CUDA_OK(cudaFuncSetAttribute(mt_horner_kernel,
           cudaFuncAttributeMaxDynamicSharedMemorySize,
-          (int) ((HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t)))))
+          (int) ((HG * HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t)))))
     return EZMOCK_ERR_UNKNOWN;
   g_mt_dev_ready = dev;
   return 0;
@@ -460,6 +466,7 @@ int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
   int e = mt_prepare(m->device);
   if (e) return e;
   // chunk length L = 2^l and number of chunks P = 2^p with P*L >= count
+  // at most 256 chunks, so every doubling level fits one wave of blocks
   int l = 12, p = 0;
   while ((1ULL << l) * 256ULL < count && l < 40) l++;
   while (((uint64_t) 1 << (l + p)) < count) p++;
@@ -481,7 +488,7 @@ int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
       !EZ_CUDA_OK(cudaMemcpyAsync(d_plist, plist.data(), plist.size() * sizeof(int),
           cudaMemcpyHostToDevice, m->stream)))
     return EZMOCK_ERR_UNKNOWN;
-  const size_t smem = (HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t);
+  const size_t smem = (HG * HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t);
   const int nbase = (int) plist.size() - p;
   // chunk 0 (state index 1) = jump of the seed window to `start`
   if (nbase > 0) {
