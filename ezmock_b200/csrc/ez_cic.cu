@@ -88,115 +88,163 @@ cic_atomic_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
 }
 
 #ifdef SINGLE_PREC
-// ---- slab kernel: shared-memory accumulation with a sliding z window ----
+// ---- owner-computes kernel (FP32) ----
 //
-// A CTA owns the particles of a 16 x 16 column of Lagrangian cells and walks
-// it along z in chunks of 8 slices.  Contributions land in a shared-memory
-// ring of 16 z slices covering the column widened by H = 2 cells on each
-// side (plus the CIC neighbour), for rho and the three momenta.  After each
-// chunk the slices no later particle can reach are added to global memory
-// with 16-byte vector atomics (4 consecutive z cells) and cleared.  Particles
-// displaced by more than H cells fall back to direct global atomics.  Needs
-// Ng a multiple of 16.
-constexpr int ST = 16;                       // column tile (x and y)
-constexpr int SH = 2;                        // halo
-constexpr int SB = ST + 2 * SH + 1;          // box side = 21
-constexpr int SKZ = 8;                       // z slices per chunk
-constexpr int SRING = 16;                    // ring length (z slices)
-constexpr int SLAB_NT = 512;
-constexpr int SQ = SB * SB * SRING;          // floats per quantity
+// A CTA owns a 16 x 16 column of output cells (all z) and walks it along z in
+// chunks of 8 slices.  For each chunk it reads every particle whose
+// Lagrangian cell lies within OH = 3 cells of the column (23 x 23 x 8
+// particles) and keeps the CIC contributions that land in its own cells, in a
+// shared-memory ring of three z chunks.  Accumulation is in 32-bit fixed
+// point (integer shared-memory atomics are exact and fast): rho in units of
+// 2^-21 per cell, the momenta in units of 2^-s with s chosen from the largest
+// |psi| so that no sum can overflow while rho < 1024.  A chunk is final once
+// the particles of the next chunk are in; it is then written with plain
+// coalesced stores, so every output cell is written exactly once and no
+// global atomics are needed.  Particles displaced by more than OH cells in
+// any direction are listed by their own CTA and deposited afterwards with
+// global atomics (fixup_kernel).  A negative rho sum (overflow) raises a flag
+// on which the host repeats the assignment with float atomics.
+constexpr int OT = 16;                       // owned column tile (x and y)
+constexpr int OH = 3;                        // halo: largest in-kernel |offset|
+constexpr int OW = OT + 2 * OH + 1;          // particle read width = 23
+constexpr int OKZ = 8;                       // z slices per chunk
+constexpr int ORS = 3 * OKZ;                 // ring: three chunks
+constexpr int OWN_NT = 512;
+constexpr int OQS = OT * OT * ORS;           // ints per quantity
+constexpr float RHO_SCALE = 2097152.f;       // 2^21
 
-__device__ __forceinline__ void gadd(real *g, real v) { atomicAdd(g, v); }
+typedef EzCicStats CicStats;
 
-__global__ void __launch_bounds__(SLAB_NT)
-cic_slab_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
+// max |psi| over the three displacement fields (for the fixed-point scale)
+__global__ void psi_absmax_kernel(const real *__restrict__ p, size_t n,
+    CicStats *stats) {
+  float mx = 0.f;
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t) gridDim.x * blockDim.x)
+    mx = fmaxf(mx, fabsf((float) p[i]));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&stats->psimax_bits, __float_as_uint(mx));
+}
+
+__global__ void __launch_bounds__(OWN_NT, 2)
+cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
     const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
-    int Ng, real igs) {
-  extern __shared__ float ring[];            // [4][SB][SB][SRING]
-  const int ntile = Ng / ST;
-  const int i0 = (blockIdx.x / ntile) * ST, j0 = (blockIdx.x % ntile) * ST;
-  for (int e = threadIdx.x; e < 4 * SQ; e += SLAB_NT) ring[e] = 0;
+    int Ng, real igs, CicStats *stats, unsigned int *list) {
+  extern __shared__ int iring[];             // [4][OT*OT][ORS]
+  const int nt = Ng / OT;
+  const int i0 = (blockIdx.x / nt) * OT, j0 = (blockIdx.x % nt) * OT;
+  // momentum scale: 1023 * max|psi| * scale < 2^31
+  const float pmax = fmaxf(__uint_as_float(stats->psimax_bits), 1e-30f);
+  const float mscale = exp2f(floorf(log2f(2147483647.f / (1024.f * pmax))));
+  const float minv = 1.f / mscale;
+  for (int e = threadIdx.x; e < 4 * OQS; e += OWN_NT) iring[e] = 0;
   __syncthreads();
-  int U = -4;                                // oldest unflushed z (multiple of 4)
-  const int nchunk = Ng / SKZ;
-  for (int c = 0; c <= nchunk; c++) {
-    if (c < nchunk) {
-      const int zc = c * SKZ;
-      for (int p = threadIdx.x; p < ST * ST * SKZ; p += SLAB_NT) {
-        const int kz = p & (SKZ - 1), tj = (p >> 3) & (ST - 1), ti = p >> 7;
-        const int i = i0 + ti, j = j0 + tj, k = zc + kz;
-        const size_t id = ((size_t) i * Ng + j) * Ng + k;
-        const real pv[3] = {p0[id], p1[id], p2[id]};
-        // positions and weights as in dens_field.c:262-289 (unwrapped cells)
-        const real x = pv[0] * igs + i, y = pv[1] * igs + j, z = pv[2] * igs + k;
-        const int x0 = (int) floor((double) x), y0 = (int) floor((double) y),
-                  z0 = (int) floor((double) z);
-        const real wx1 = x - x0, wx0 = 1 - wx1;
-        const real wy1 = y - y0, wy0 = 1 - wy1;
-        const real wz1 = z - z0, wz0 = 1 - wz1;
-        const int rx = x0 - (i0 - SH), ry = y0 - (j0 - SH);
-        const bool inbox = rx >= 0 && rx <= SB - 2 && ry >= 0 && ry <= SB - 2 &&
-            z0 >= zc - SH && z0 <= zc + SKZ - 1 + SH;
-        const real wxs[2] = {wx0, wx1}, wys[2] = {wy0, wy1}, wzs[2] = {wz0, wz1};
-        if (inbox) {
+  const int nch = Ng / OKZ;
+  const int lane = threadIdx.x & 31;
+  for (int c = -1; c <= nch; c++) {
+    for (int p = threadIdx.x; p < OW * OW * OKZ; p += OWN_NT) {
+      const int kz = p & (OKZ - 1), lc = p >> 3;
+      const int lj = lc % OW, li = lc / OW;
+      const int iu = i0 - OH + li, ju = j0 - OH + lj, zu = c * OKZ + kz;
+      const int iw = (iu + Ng) % Ng, jw = (ju + Ng) % Ng, zw = (zu + Ng) % Ng;
+      const size_t id = ((size_t) iw * Ng + jw) * Ng + zw;
+      const real pv[3] = {p0[id], p1[id], p2[id]};
+      // positions and weights exactly as dens_field.c:262-275
+      const real x = pv[0] * igs + iw, y = pv[1] * igs + jw, z = pv[2] * igs + zw;
+      const int x0 = (int) floor((double) x), y0 = (int) floor((double) y),
+                z0 = (int) floor((double) z);
+      const real wx1 = x - x0, wx0 = 1 - wx1;
+      const real wy1 = y - y0, wy0 = 1 - wy1;
+      const real wz1 = z - z0, wz0 = 1 - wz1;
+      const int dx = x0 - iw, dy = y0 - jw, dz = z0 - zw;
+      const bool far = dx < -OH || dx > OH || dy < -OH || dy > OH || dz < -OH || dz > OH;
+      const bool own = li >= OH && li < OH + OT && lj >= OH && lj < OH + OT && c >= 0 && c < nch;
+      const unsigned am = __activemask();
+      const unsigned fm = __ballot_sync(am, far && own);
+      if (fm) {
+        const int leader = __ffs(fm) - 1;
+        unsigned int base = 0;
+        if (lane == leader) base = atomicAdd(&stats->nlist, (unsigned) __popc(fm));
+        base = __shfl_sync(am, base, leader);
+        if (far && own) list[base + __popc(fm & ((1u << lane) - 1))] = (unsigned int) id;
+      }
+      if (far) continue;
+      const real wxs[2] = {wx0, wx1}, wys[2] = {wy0, wy1}, wzs[2] = {wz0, wz1};
 #pragma unroll
-          for (int a = 0; a < 2; a++)
+      for (int a = 0; a < 2; a++) {
+        const int cx = li - OH + dx + a;
+        if (cx < 0 || cx >= OT) continue;
 #pragma unroll
-            for (int b = 0; b < 2; b++)
+        for (int b = 0; b < 2; b++) {
+          const int cy = lj - OH + dy + b;
+          if (cy < 0 || cy >= OT) continue;
 #pragma unroll
-              for (int cz = 0; cz < 2; cz++) {
-                const int base = ((rx + a) * SB + (ry + b)) * SRING + ((z0 + cz) & (SRING - 1));
-                const real w = wxs[a] * wys[b] * wzs[cz];
-                atomicAdd(ring + base, (float) w);
+          for (int cz = 0; cz < 2; cz++) {
+            const int zz = zu + dz + cz;
+            if (zz < 0 || zz >= Ng) continue;
+            const int slot = ((zz >> 3) % 3) * OKZ + (zz & (OKZ - 1));
+            const int base = (cx * OT + cy) * ORS + slot;
+            atomicAdd(iring + base, __float2int_rn(wxs[a] * wys[b] * wzs[cz] * RHO_SCALE));
 #pragma unroll
-                for (int d = 0; d < 3; d++)
-                  atomicAdd(ring + (d + 1) * SQ + base, (float) ((wxs[a] * pv[d]) * wys[b] * wzs[cz]));
-              }
-        }
-        else {
-          int xs[2], ys[2], zs[2];
-          xs[0] = ((x0 % Ng) + Ng) % Ng; xs[1] = (xs[0] == Ng - 1) ? 0 : xs[0] + 1;
-          ys[0] = ((y0 % Ng) + Ng) % Ng; ys[1] = (ys[0] == Ng - 1) ? 0 : ys[0] + 1;
-          zs[0] = ((z0 % Ng) + Ng) % Ng; zs[1] = (zs[0] == Ng - 1) ? 0 : zs[0] + 1;
-#pragma unroll
-          for (int a = 0; a < 2; a++)
-#pragma unroll
-            for (int b = 0; b < 2; b++)
-#pragma unroll
-              for (int cz = 0; cz < 2; cz++) {
-                const size_t g = ((size_t) xs[a] * Ng + ys[b]) * Ng + zs[cz];
-                gadd(rho + g, wxs[a] * wys[b] * wzs[cz]);
-                gadd(q0 + g, (wxs[a] * pv[0]) * wys[b] * wzs[cz]);
-                gadd(q1 + g, (wxs[a] * pv[1]) * wys[b] * wzs[cz]);
-                gadd(q2 + g, (wxs[a] * pv[2]) * wys[b] * wzs[cz]);
-              }
+            for (int d = 0; d < 3; d++)
+              atomicAdd(iring + (d + 1) * OQS + base,
+                  __float2int_rn((wxs[a] * pv[d]) * wys[b] * wzs[cz] * mscale));
+          }
         }
       }
     }
     __syncthreads();
-    // flush the quads of z slices no later particle can reach
-    const int zfinal = (c < nchunk) ? (c + 1) * SKZ - SH : Ng + SH + 2;
-    int nq = 0;
-    while (U + 4 * (nq + 1) <= zfinal) nq++;
-    const int ntask = nq * 4 * SB * SB;
-    for (int t = threadIdx.x; t < ntask; t += SLAB_NT) {
-      const int qd = t / (4 * SB * SB);
-      const int r = t - qd * 4 * SB * SB;
-      const int q = r / (SB * SB), col = r - q * SB * SB;
-      const int rx = col / SB, ry = col - rx * SB;
-      const int zq = U + 4 * qd;
-      float4 *src = (float4 *) (ring + q * SQ + col * SRING + (zq & (SRING - 1)));
-      const float4 v = *src;
-      *src = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
-      const int gx = (((i0 - SH + rx) % Ng) + Ng) % Ng;
-      const int gy = (((j0 - SH + ry) % Ng) + Ng) % Ng;
-      const int gz = ((zq % Ng) + Ng) % Ng;
-      real *gq = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
-      atomicAdd((float4 *) (gq + ((size_t) gx * Ng + gy) * Ng + gz), v);
+    const int o = c - 1;                     // output chunk now complete
+    if (o >= 0 && o < nch) {
+      for (int t = threadIdx.x; t < 4 * OT * OT * OKZ; t += OWN_NT) {
+        const int s = t & (OKZ - 1), col = (t >> 3) % (OT * OT), q = t / (OT * OT * OKZ);
+        const int idx = q * OQS + col * ORS + (o % 3) * OKZ + s;
+        const int v = iring[idx];
+        iring[idx] = 0;
+        if (q == 0 && v < 0) stats->overflow = 1;
+        real *g = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
+        const int cx = col / OT, cy = col - cx * OT;
+        g[((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + o * OKZ + s] =
+            (q == 0) ? (real) v * (1.f / RHO_SCALE) : (real) v * minv;
+      }
     }
-    U += 4 * nq;
     __syncthreads();
+  }
+}
+
+// Deposits the listed far-displaced particles with global atomics.
+__global__ void __launch_bounds__(CIC_NT)
+fixup_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
+    const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
+    int Ng, real igs, const CicStats *stats, const unsigned int *list) {
+  const unsigned int n = stats->nlist;
+  for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += gridDim.x * blockDim.x) {
+    const size_t id = list[t];
+    const int k = (int) (id % Ng);
+    const size_t ij = id / Ng;
+    const int j = (int) (ij % Ng), i = (int) (ij / Ng);
+    const real pv[3] = {p0[id], p1[id], p2[id]};
+    int x0, x1, y0, y1, z0, z1;
+    real wx0, wx1, wy0, wy1, wz0, wz1;
+    cic_axis(pv[0], igs, i, Ng, &x0, &x1, &wx0, &wx1);
+    cic_axis(pv[1], igs, j, Ng, &y0, &y1, &wy0, &wy1);
+    cic_axis(pv[2], igs, k, Ng, &z0, &z1, &wz0, &wz1);
+    const int xs[2] = {x0, x1}, ys[2] = {y0, y1}, zs[2] = {z0, z1};
+    const real wxs[2] = {wx0, wx1}, wys[2] = {wy0, wy1}, wzs[2] = {wz0, wz1};
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+      for (int b = 0; b < 2; b++)
+#pragma unroll
+        for (int cz = 0; cz < 2; cz++) {
+          const size_t g = idx3(Ng, xs[a], ys[b], zs[cz]);
+          atomicAdd(rho + g, wxs[a] * wys[b] * wzs[cz]);
+          atomicAdd(q0 + g, (wxs[a] * pv[0]) * wys[b] * wzs[cz]);
+          atomicAdd(q1 + g, (wxs[a] * pv[1]) * wys[b] * wzs[cz]);
+          atomicAdd(q2 + g, (wxs[a] * pv[2]) * wys[b] * wzs[cz]);
+        }
   }
 }
 #endif
@@ -277,25 +325,46 @@ int ez_cic(EzMesh *m, double Lbox) {
         m->paint[1], m->paint[2], N); ez_count_launch();
   }
   else {
-    if (!EZ_CUDA_OK(cudaMemsetAsync(m->rho, 0, N * sizeof(real), m->stream))) return EZMOCK_ERR_UNKNOWN;
-    for (int d = 0; d < 3; d++)
-      if (!EZ_CUDA_OK(cudaMemsetAsync(m->paint[d], 0, N * sizeof(real), m->stream)))
-        return EZMOCK_ERR_UNKNOWN;
 #ifdef SINGLE_PREC
-    if (Ng % ST == 0 && Ng >= 2 * ST) {
+    if (Ng % OT == 0 && Ng >= 2 * OT) {
       static bool attr = false;
-      const size_t smem = 4 * SQ * sizeof(float);
+      const size_t smem = 4 * OQS * sizeof(int);
       if (!attr) {
-        cudaFuncSetAttribute(cic_slab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaFuncSetAttribute(cic_owner_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
         attr = true;
       }
-      cic_slab_kernel<<<(unsigned) ((Ng / ST) * (Ng / ST)), SLAB_NT, smem, m->stream>>>(
+      CicStats *stats = (CicStats *) m->stats;
+      unsigned int *list = m->draws;                  // free after the spectrum
+      if (!m->psimax_valid) {
+        cudaMemsetAsync(&stats->psimax_bits, 0, sizeof(unsigned int), m->stream);
+        psi_absmax_kernel<<<148 * 8, 256, 0, m->stream>>>(m->psi[0], 3 * N, stats); ez_count_launch();
+      }
+      cudaMemsetAsync(&stats->nlist, 0, 2 * sizeof(int), m->stream);
+      cic_owner_kernel<<<(unsigned) ((Ng / OT) * (Ng / OT)), OWN_NT, smem, m->stream>>>(
           m->psi[0], m->psi[1], m->psi[2], m->rho, m->paint[0], m->paint[1],
-          m->paint[2], Ng, igs); ez_count_launch();
+          m->paint[2], Ng, igs, stats, list); ez_count_launch();
+      fixup_kernel<<<148 * 4, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
+          m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs,
+          stats, list); ez_count_launch();
+      int ovf = 0;
+      if (!EZ_CUDA_OK(cudaMemcpyAsync(&ovf, &stats->overflow, sizeof(int), cudaMemcpyDeviceToHost, m->stream)) ||
+          !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
+        return EZMOCK_ERR_UNKNOWN;
+      if (ovf) {
+        // a cell holds >= 1024 particles: repeat with float atomics
+        cudaMemsetAsync(m->rho, 0, N * sizeof(real), m->stream);
+        for (int d = 0; d < 3; d++) cudaMemsetAsync(m->paint[d], 0, N * sizeof(real), m->stream);
+        cic_atomic_kernel<true><<<grid, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
+            m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, N); ez_count_launch();
+      }
     }
     else
 #endif
     {
+      if (!EZ_CUDA_OK(cudaMemsetAsync(m->rho, 0, N * sizeof(real), m->stream))) return EZMOCK_ERR_UNKNOWN;
+      for (int d = 0; d < 3; d++)
+        if (!EZ_CUDA_OK(cudaMemsetAsync(m->paint[d], 0, N * sizeof(real), m->stream)))
+          return EZMOCK_ERR_UNKNOWN;
       cic_atomic_kernel<true><<<grid, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
           m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, N); ez_count_launch();
     }

@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(FFT_NT)
 fft_pass_k(const cplx *__restrict__ s0, const cplx *__restrict__ s1,
     const cplx *__restrict__ s2, real *__restrict__ p0, real *__restrict__ p1,
     real *__restrict__ p2, int Ng, int Nkp, int R, size_t nrows,
-    FftPlanDev pl, const cplx *__restrict__ twg) {
+    FftPlanDev pl, const cplx *__restrict__ twg, EzCicStats *stats) {
   extern __shared__ unsigned char smraw[];
   const int Nh = Ng >> 1;
   const int nl = 3 * R;
@@ -288,6 +288,7 @@ fft_pass_k(const cplx *__restrict__ s0, const cplx *__restrict__ s1,
   }
   __syncthreads();
   cplx *res = smem_fft<1>(ba, bb, nl, pl, tw);
+  float mx = 0.f;
   for (int e = threadIdx.x; e < nl * Nh; e += blockDim.x) {
     const int L = e / Nh, m = e - L * Nh;
     const int r = L / 3, comp = L - 3 * r;
@@ -297,7 +298,12 @@ fft_pass_k(const cplx *__restrict__ s0, const cplx *__restrict__ s1,
     const cplx z = res[m * nl + L];
     cplx *d2 = (cplx *) (dst + row * Ng);
     d2[m] = z;
+    mx = fmaxf(mx, fmaxf(fabsf((float) z.x), fabsf((float) z.y)));
   }
+  // max |psi|, for the fixed-point scale of the density assignment
+#pragma unroll
+  for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&stats->psimax_bits, __float_as_uint(mx));
 }
 
 // ------------------------------------------- forward transforms (r2c) ---
@@ -476,11 +482,13 @@ int ez_fft_c2r_psi(EzMesh *m) {
       m->spec[2], Ng, Nkp, K, pn); ez_count_launch();
   ez_stage_end(m, ST_FFT_J);
   const size_t nrows = (size_t) Ng * Ng;
+  cudaMemsetAsync(&((EzCicStats *) m->stats)->psimax_bits, 0, sizeof(unsigned int), m->stream);
   ez_stage_begin(m, ST_FFT_K);
   fft_pass_k<<<(unsigned) ((nrows + R - 1) / R), FFT_NT, sm_k, m->stream>>>(
       m->spec[0], m->spec[1], m->spec[2], m->psi[0], m->psi[1], m->psi[2], Ng,
-      Nkp, R, nrows, ph, twg); ez_count_launch();
+      Nkp, R, nrows, ph, twg, (EzCicStats *) m->stats); ez_count_launch();
   ez_stage_end(m, ST_FFT_K);
+  m->psimax_valid = true;
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 

@@ -146,6 +146,7 @@ void mesh_free_device(EzMesh *m) {
   if (m->scratch) cudaFree(m->scratch);
   if (m->rng_scratch) cudaFree(m->rng_scratch);
   if (m->fixacc) cudaFree(m->fixacc);
+  if (m->stats) cudaFree(m->stats);
   if (m->cat) cudaFree(m->cat);
   if (m->h_stage) cudaFreeHost(m->h_stage);
   if (m->stream) cudaStreamDestroy(m->stream);
@@ -260,13 +261,18 @@ int ez_scratch(EzMesh *m, size_t bytes) {
   return 0;
 }
 
+// Grows the RNG scratch, keeping its contents (prepared stream states).
 int ez_rng_scratch(EzMesh *m, size_t bytes) {
   if (bytes <= m->rng_scratch_cap) return 0;
-  if (m->rng_scratch) cudaFree(m->rng_scratch);
-  m->rng_scratch = nullptr;
-  m->rng_scratch_cap = 0;
   bytes = (bytes + 4095) / 4096 * 4096;
-  if (!EZ_CUDA_OK(cudaMalloc(&m->rng_scratch, bytes))) return EZMOCK_ERR_MEMORY;
+  void *p = nullptr;
+  if (!EZ_CUDA_OK(cudaMalloc(&p, bytes))) return EZMOCK_ERR_MEMORY;
+  if (m->rng_scratch) {
+    cudaMemcpyAsync(p, m->rng_scratch, m->rng_scratch_cap, cudaMemcpyDeviceToDevice, m->stream);
+    cudaStreamSynchronize(m->stream);
+    cudaFree(m->rng_scratch);
+  }
+  m->rng_scratch = p;
   m->rng_scratch_cap = bytes;
   return 0;
 }
@@ -313,6 +319,8 @@ int ez_mesh_alloc(EzMesh *m, int Ng) {
     return EZMOCK_ERR_MEMORY;
   }
   m->draws_cap = ndraw;
+  if (!EZ_CUDA_OK(cudaMalloc(&m->stats, sizeof(EzCicStats)))) return EZMOCK_ERR_MEMORY;
+  cudaMemset(m->stats, 0, sizeof(EzCicStats));
   for (int d = 0; d < 3; d++) {
     m->spec[d] = spec + d * m->Nspec;
     m->psi[d] = psi + d * m->N;
@@ -503,6 +511,7 @@ int EZmock_create_dens_field(EZMOCK *ez, real *psi[3], bool deepcopy,
   if ((e = set_device(m))) return (*err = e);
   for (int s = 0; s < ST_NSTAGE; s++) m->ev_used[s] = false;
   m->have_field = false;
+  m->psimax_valid = false;
   const size_t bytes = m->N * sizeof(real);
   if (user_psi) {
     // dens_field.c:351-374: the displacements are taken as given
@@ -523,6 +532,7 @@ int EZmock_create_dens_field(EZMOCK *ez, real *psi[3], bool deepcopy,
         return (*err = e);
       const real norm = 1 / sqrt((double) m->N);
       if ((e = ez_scale_psi(m, norm))) return (*err = e);
+      m->psimax_valid = false;
     }
     else {
       const size_t ndraw = ((size_t) conf->Ng * conf->Ng * m->Nk - 1) * (fixamp ? 1 : 2);

@@ -98,12 +98,25 @@ struct EzMesh {
   size_t scratch_cap;
   void *rng_scratch;       // skip-ahead states of the MT19937 streams
   size_t rng_scratch_cap;
+  struct { uint64_t start, cap; int l, p; size_t first; } rng_prep[4];
+  int rng_nprep;           // prepared stream ranges (ez_rng_prepare)
+  size_t rng_prep_end;     // first free state slot after them
   unsigned long long *fixacc;   // deterministic CIC accumulators (4 x N)
+  void *stats;             // EzCicStats on the device
+  bool psimax_valid;       // stats->psimax_bits holds max |psi| of the fields
   real *cat;               // device catalogue (6 x cap)
   size_t cat_cap;
   size_t cat_n;            // length of the last catalogue (array stride)
   real *h_stage;           // pinned host staging for the catalogue
   size_t h_stage_cap;
+};
+
+// Device-side statistics of the displacement/density assignment.
+struct EzCicStats {
+  unsigned int psimax_bits;   // max |psi| over the three fields (float bits)
+  unsigned int nlist;         // far-displaced particles listed for fixup
+  int overflow;               // a fixed-point cell sum overflowed
+  int pad;
 };
 
 // ---- error helpers ----
@@ -112,6 +125,14 @@ struct EzMesh {
 // ---- RNG (ez_rng.cu) ----
 // Raw 32-bit draws [start, start+count) of the stream seeded by `seed`.
 int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
+    uint64_t count, uint32_t *out);
+// Prepares the ranges [starts[i], starts[i] + caps[i]) of one stream so that
+// later fills of them skip the jump (MT19937 chunk states computed together).
+#define EZ_RNG_MAXPREP 4
+int ez_rng_prepare(EzMesh *m, int ran, uint64_t seed, const uint64_t *starts,
+    const uint64_t *caps, int n);
+// Draws [starts[i], starts[i] + count) of prepared range i.
+int ez_rng_fill_prepared(EzMesh *m, int ran, uint64_t seed, int i,
     uint64_t count, uint32_t *out);
 // Conversions shared by all kernels (prand definitions of the oracle):
 //   MT19937  : u = x 2^-32 in [0,1); u_pos = (x + 0.5) 2^-32 in (0,1)

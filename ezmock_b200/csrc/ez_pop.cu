@@ -664,6 +664,14 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   real *rhot = (real *) m->spec[0];
   cudaStream_t st = m->stream;
 
+  // random streams of the three stages, prepared together (MT19937 jumps)
+  {
+    const uint64_t nt_cap = ntot + ntot / 32 + 1024;
+    const uint64_t starts[3] = {(uint64_t) N << 1, (uint64_t) N * 5, (uint64_t) N << 3};
+    const uint64_t caps[3] = {(uint64_t) N + 2, 3 * nt_cap, 6 * ((nt_cap + 1) / 2)};
+    if ((e = ez_rng_prepare(m, ran, seed, starts, caps, 3))) return e;
+  }
+
   // ---- 1. valid ranks ----
   ez_stage_begin(m, ST_BIAS);
   valid_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, N, thres, bcnt); ez_count_launch();
@@ -678,7 +686,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // ---- 2. bias ----
   const size_t nd_bias = nvalid + (nvalid & 1);
   if ((e = ensure_draws(m, std::max(nd_bias, (size_t) 1)))) return e;
-  if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N << 1, nd_bias, m->draws))) return e;
+  if ((e = ez_rng_fill_prepared(m, ran, seed, 0, nd_bias, m->draws))) return e;
   cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
   bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
       (double) (real) EZ_GAUSS_WIDTH, bscan, m->draws, ran, hist); ez_count_launch();
@@ -719,7 +727,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // the per-cell counts must add up to the selected total (pop_tracer.c:989-993)
   if (ncount != nt_all) { res->err = EZMOCK_ERR_UNKNOWN; return 0; }
   if ((e = ensure_draws(m, std::max((size_t) 3 * nt_all, (size_t) 1)))) return e;
-  if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N * 5, 3 * nt_all, m->draws))) return e;
+  if ((e = ez_rng_fill_prepared(m, ran, seed, 1, 3 * nt_all, m->draws))) return e;
   const real gs = Lbox / Ng;
   emit_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, Ng, bo, bscan, m->draws,
       ran, gs, Lbox, (unsigned long long) nt_all, cx, cy, cz); ez_count_launch();
@@ -732,7 +740,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
       m->paint[1], m->paint[2], Ng, igs, vfac, nt_all, cx, cy, cz, cvx, cvy, cvz); ez_count_launch();
   const size_t nd_disp = 6 * ((nt_all + 1) / 2);
   if ((e = ensure_draws(m, std::max(nd_disp, (size_t) 1)))) return e;
-  if ((e = ez_rng_fill(m, ran, seed, (uint64_t) N << 3, nd_disp, m->draws))) return e;
+  if ((e = ez_rng_fill_prepared(m, ran, seed, 2, nd_disp, m->draws))) return e;
   disp_kernel<<<grid_for((nt_all + 1) / 2, NT), NT, 0, st>>>(nt_all, m->draws,
       ran, (double) sigma_v, cvx, cvy, cvz); ez_count_launch();
   ez_stage_end(m, ST_VEL);

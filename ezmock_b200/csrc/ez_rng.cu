@@ -24,6 +24,7 @@
 //    is then generated by one block with the three-phase twist.
 #include "ez_internal.cuh"
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -231,17 +232,23 @@ __device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
 // 16-bit windows of p: r <- T^16 r + sum_g tab_g[c_g], where tab_g[c] =
 // sum_{j<4} c_j T^(4g+j) s are four 16-entry tables of combinations of the
 // source state (shared memory), so each window costs one barrier.
+// Block b applies desc[b] = {in state, out state, first poly, npoly}.
 __global__ void __launch_bounds__(H_THREADS)
-mt_horner_kernel(const uint32_t *__restrict__ states_in, uint32_t *states_out,
-    size_t in_base, size_t out_base, const uint64_t *__restrict__ polys,
-    const int *__restrict__ plist, int npoly) {
+mt_horner_kernel(uint32_t *states, const int4 *__restrict__ desc,
+    const uint64_t *__restrict__ polys, const int *__restrict__ plist_all) {
   extern __shared__ uint32_t sm[];
+  const int4 dsc = desc[blockIdx.x];
+  const size_t in_base = (size_t) dsc.x, out_base = (size_t) dsc.y;
+  const int *plist = plist_all + dsc.z;
+  const int npoly = dsc.w;
+  const uint32_t *states_in = states;
+  uint32_t *states_out = states;
   uint32_t *tab = sm;                        // HG x HTAB x MT_N
   uint32_t *ext = tab + HG * HTAB * MT_N;    // MT_N + HW
   uint32_t *ra = ext + MT_N + HW;            // MT_N
   uint32_t *rb = ra + MT_N;                  // MT_N
   const int t = threadIdx.x;
-  const uint32_t *src = states_in + (in_base + blockIdx.x) * MT_N;
+  const uint32_t *src = states_in + in_base * MT_N;
   for (int k = t; k < MT_N; k += blockDim.x) ext[k] = src[k];
   __syncthreads();
   for (int ip = 0; ip < npoly; ip++) {
@@ -282,7 +289,7 @@ mt_horner_kernel(const uint32_t *__restrict__ states_in, uint32_t *states_out,
     for (int k = t; k < MT_N; k += blockDim.x) ext[k] = r0[k];
     __syncthreads();
   }
-  uint32_t *dst = states_out + (out_base + blockIdx.x) * MT_N;
+  uint32_t *dst = states_out + out_base * MT_N;
   for (int k = t; k < MT_N; k += blockDim.x) dst[k] = ext[k];
 }
 
@@ -460,52 +467,117 @@ int mt_prepare(int dev) {
   return 0;
 }
 
-int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
-    uint32_t *out) {
-  if (!count) return 0;
+// A range of one stream: chunk c starts at draw `start + c L` (L = 2^l,
+// c < P = 2^p); its window is states[first + c].
+struct MtRange {
+  uint64_t start, cap;
+  int l, p;
+  size_t first;
+};
+
+MtRange mt_plan(uint64_t start, uint64_t cap) {
+  // at most 128 chunks per range, so a doubling level over three ranges
+  // stays within a few waves of blocks
+  MtRange r;
+  r.start = start;
+  r.cap = cap;
+  r.l = 12;
+  r.p = 0;
+  while ((1ULL << r.l) * 128ULL < cap && r.l < 40) r.l++;
+  while (((uint64_t) 1 << (r.l + r.p)) < cap) r.p++;
+  r.first = 0;
+  return r;
+}
+
+// Chunk states of `nr` ranges of the stream seeded by `seed`, computed
+// together: one launch for the jumps to the range starts, then one launch per
+// doubling level covering all ranges.  State 0 is the seed window; the
+// states live at `base` in the RNG scratch.
+int mt_prepare_ranges(EzMesh *m, uint64_t seed, MtRange *r, int nr,
+    size_t base) {
   int e = mt_prepare(m->device);
   if (e) return e;
-  // chunk length L = 2^l and number of chunks P = 2^p with P*L >= count
-  // at most 256 chunks, so every doubling level fits one wave of blocks
-  int l = 12, p = 0;
-  while ((1ULL << l) * 256ULL < count && l < 40) l++;
-  while (((uint64_t) 1 << (l + p)) < count) p++;
-  const uint64_t L = 1ULL << l;
-  const uint64_t P = 1ULL << p;
-  // scratch: P states + seed state + polynomial index list
+  size_t nst = 1;
+  int pmax = 0;
+  for (int i = 0; i < nr; i++) {
+    r[i].first = base + nst;
+    nst += (size_t) 1 << r[i].p;
+    pmax = std::max(pmax, r[i].p);
+  }
   std::vector<int> plist;
-  for (int k = 0; k < 64; k++)
-    if ((start >> k) & 1ULL) plist.push_back(k);
-  for (int lev = 0; lev < p; lev++) plist.push_back(l + lev);
-  const size_t st_bytes = (size_t) (P + 1) * MT_N * sizeof(uint32_t);
-  const size_t need = st_bytes + plist.size() * sizeof(int) + 256;
+  std::vector<int4> desc;
+  std::vector<int> lev_off(pmax + 2), lev_n(pmax + 2);
+  lev_off[0] = 0;
+  for (int i = 0; i < nr; i++) {          // level "base": seed -> range start
+    int4 d;
+    d.x = (int) base;
+    d.y = (int) r[i].first;
+    d.z = (int) plist.size();
+    for (int k = 0; k < 64; k++)
+      if ((r[i].start >> k) & 1ULL) plist.push_back(k);
+    d.w = (int) plist.size() - d.z;
+    desc.push_back(d);
+  }
+  lev_n[0] = nr;
+  for (int lev = 0; lev < pmax; lev++) {
+    lev_off[lev + 1] = (int) desc.size();
+    for (int i = 0; i < nr; i++) {
+      if (lev >= r[i].p) continue;
+      const int pk = (int) plist.size();
+      plist.push_back(r[i].l + lev);
+      for (int t = 0; t < (1 << lev); t++) {
+        int4 d;
+        d.x = (int) (r[i].first + t);
+        d.y = (int) (r[i].first + t + (1 << lev));
+        d.z = pk;
+        d.w = 1;
+        desc.push_back(d);
+      }
+    }
+    lev_n[lev + 1] = (int) desc.size() - lev_off[lev + 1];
+  }
+  const size_t st_bytes = (base + nst) * MT_N * sizeof(uint32_t);
+  const size_t d_bytes = desc.size() * sizeof(int4);
+  const size_t need = st_bytes + d_bytes + plist.size() * sizeof(int) + 512;
   if ((e = ez_rng_scratch(m, need))) return e;
-  uint32_t *states = (uint32_t *) m->rng_scratch;    // [0]: seed, [1..P]: chunks
-  int *d_plist = (int *) ((char *) m->rng_scratch + st_bytes);
+  uint32_t *states = (uint32_t *) m->rng_scratch;
+  int4 *d_desc = (int4 *) ((char *) m->rng_scratch + (st_bytes + 15) / 16 * 16);
+  int *d_plist = (int *) ((char *) d_desc + d_bytes);
   std::vector<uint32_t> w(MT_N);
   mt_seed_window(seed, w.data());
-  if (!EZ_CUDA_OK(cudaMemcpyAsync(states, w.data(), MT_N * 4, cudaMemcpyHostToDevice, m->stream)) ||
-      !EZ_CUDA_OK(cudaMemcpyAsync(d_plist, plist.data(), plist.size() * sizeof(int),
-          cudaMemcpyHostToDevice, m->stream)))
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(states + base * MT_N, w.data(), MT_N * 4,
+          cudaMemcpyHostToDevice, m->stream)) ||
+      !EZ_CUDA_OK(cudaMemcpyAsync(d_desc, desc.data(), d_bytes, cudaMemcpyHostToDevice, m->stream)) ||
+      (plist.size() && !EZ_CUDA_OK(cudaMemcpyAsync(d_plist, plist.data(),
+          plist.size() * sizeof(int), cudaMemcpyHostToDevice, m->stream))))
     return EZMOCK_ERR_UNKNOWN;
   const size_t smem = (HG * HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t);
-  const int nbase = (int) plist.size() - p;
-  // chunk 0 (state index 1) = jump of the seed window to `start`
-  if (nbase > 0) {
-    mt_horner_kernel<<<1, H_THREADS, smem, m->stream>>>(states, states, 0, 1,
-        g_mt_xpow_dev, d_plist, nbase); ez_count_launch();
+  for (int lev = 0; lev <= pmax; lev++) {
+    if (!lev_n[lev]) continue;
+    mt_horner_kernel<<<lev_n[lev], H_THREADS, smem, m->stream>>>(states,
+        d_desc + lev_off[lev], g_mt_xpow_dev, d_plist); ez_count_launch();
   }
-  else {
-    cudaMemcpyAsync(states + MT_N, states, MT_N * 4, cudaMemcpyDeviceToDevice, m->stream);
-  }
-  for (int lev = 0; lev < p; lev++) {
-    const unsigned nb = 1u << lev;
-    mt_horner_kernel<<<nb, H_THREADS, smem, m->stream>>>(states, states, 1,
-        1 + nb, g_mt_xpow_dev, d_plist + nbase + lev, 1); ez_count_launch();
-  }
-  mt_gen_kernel<<<(unsigned) P, G_THREADS, 0, m->stream>>>(states + MT_N, L,
-      count, out); ez_count_launch();
+  // (copies from pageable host memory are staged before cudaMemcpyAsync
+  // returns, so the host vectors may be released here)
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+int mt_generate(EzMesh *m, const MtRange &r, uint64_t count, uint32_t *out) {
+  if (!count) return 0;
+  const uint32_t *states = (const uint32_t *) m->rng_scratch + r.first * MT_N;
+  const uint64_t L = 1ULL << r.l;
+  const unsigned nb = (unsigned) ((count + L - 1) / L);
+  mt_gen_kernel<<<nb, G_THREADS, 0, m->stream>>>(states, L, count, out); ez_count_launch();
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
+    uint32_t *out, size_t base) {
+  if (!count) return 0;
+  MtRange r = mt_plan(start, count);
+  int e = mt_prepare_ranges(m, seed, &r, 1, base);
+  if (e) return e;
+  return mt_generate(m, r, count, out);
 }
 
 // Host copy of the seeding, used for the MT19937 raw-output check below.
@@ -513,6 +585,51 @@ int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
 
 int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
     uint64_t count, uint32_t *out) {
-  if (ran == EZMOCK_RNG_MT19937) return mt_fill(m, seed, start, count, out);
+  m->rng_nprep = 0;                         // the scratch is reused
+  if (ran == EZMOCK_RNG_MT19937) return mt_fill(m, seed, start, count, out, 0);
   return mrg_fill(m, seed, start, count, out);
+}
+
+int ez_rng_prepare(EzMesh *m, int ran, uint64_t seed, const uint64_t *starts,
+    const uint64_t *caps, int n) {
+  m->rng_nprep = 0;
+  if (n > EZ_RNG_MAXPREP) return EZMOCK_ERR_UNKNOWN;
+  for (int i = 0; i < n; i++) {
+    m->rng_prep[i].start = starts[i];
+    m->rng_prep[i].cap = caps[i];
+  }
+  if (ran == EZMOCK_RNG_MT19937) {
+    MtRange r[EZ_RNG_MAXPREP];
+    for (int i = 0; i < n; i++) r[i] = mt_plan(starts[i], caps[i] ? caps[i] : 1);
+    const int e = mt_prepare_ranges(m, seed, r, n, 0);
+    if (e) return e;
+    size_t end = 0;
+    for (int i = 0; i < n; i++) {
+      m->rng_prep[i].l = r[i].l;
+      m->rng_prep[i].p = r[i].p;
+      m->rng_prep[i].first = r[i].first;
+      end = std::max(end, r[i].first + ((size_t) 1 << r[i].p));
+    }
+    m->rng_prep_end = end;
+  }
+  m->rng_nprep = n;
+  return 0;
+}
+
+int ez_rng_fill_prepared(EzMesh *m, int ran, uint64_t seed, int i,
+    uint64_t count, uint32_t *out) {
+  if (i >= m->rng_nprep || count > m->rng_prep[i].cap || ran != EZMOCK_RNG_MT19937) {
+    if (ran == EZMOCK_RNG_MT19937)
+      // beyond the prepared capacity: states after the prepared ones
+      return mt_fill(m, seed, m->rng_prep[i < m->rng_nprep ? i : 0].start, count, out,
+          m->rng_nprep ? m->rng_prep_end : 0);
+    return mrg_fill(m, seed, m->rng_prep[i].start, count, out);
+  }
+  MtRange r;
+  r.start = m->rng_prep[i].start;
+  r.cap = m->rng_prep[i].cap;
+  r.l = m->rng_prep[i].l;
+  r.p = m->rng_prep[i].p;
+  r.first = m->rng_prep[i].first;
+  return mt_generate(m, r, count, out);
 }
