@@ -15,6 +15,24 @@ from . import _lib
 
 __all__ = ["EZmock"]
 
+_libc = ctypes.CDLL(None)
+_libc.free.argtypes = [ctypes.c_void_p]
+_libc.free.restype = None
+
+
+def _owned_array(ptr, n, ctype):
+    """numpy view of n `ctype` values at a malloc()'d pointer; the memory is
+    released with free() once the array (and every view of it) is gone."""
+    import weakref
+    addr = ctypes.cast(ptr, ctypes.c_void_p).value
+    if not n:
+        _libc.free(addr)
+        return np.zeros(0, np.dtype(ctype))
+    buf = (ctype * n).from_address(addr)
+    arr = np.frombuffer(buf, dtype=np.dtype(ctype))
+    weakref.finalize(buf, _libc.free, addr)
+    return arr
+
 
 class EZmock:
     def __init__(self, *args, prec=32, **kwargs):
@@ -135,17 +153,11 @@ class EZmock:
         self._assert_return_value()
         return num.value, ptrs
 
-    # -- EZmock.pyx:337-405
+    # -- EZmock.pyx:337-405: the arrays own the library's malloc() memory
+    #    (no copy), released with free() when numpy drops them
     def populate_tracer(self, rho_c, rho_exp, pdf_base, sigma_v, ntracer, att_part=False):
         n, ptrs = self._populate(rho_c, rho_exp, pdf_base, sigma_v, ntracer, att_part)
-        libc = ctypes.CDLL(None)
-        libc.free.argtypes = [ctypes.c_void_p]
-        out = []
-        for p in ptrs:
-            arr = np.ctypeslib.as_array(p, shape=(n,)).copy() if n else np.zeros(0, self._rdt)
-            libc.free(ctypes.cast(p, ctypes.c_void_p))
-            out.append(arr)
-        return tuple(out)
+        return tuple(_owned_array(p, n, self._L._rt) for p in ptrs)
 
     # -- EZmock.pyx:408-485
     def populate_tracer_to_file(self, rho_c, rho_exp, pdf_base, sigma_v, ntracer, fname,

@@ -10,8 +10,10 @@
 // matters and is kept.
 //
 // Three HBM passes, each a batch of 1D transforms staged through shared
-// memory (Stockham autosort, radices 8/4/2/3/5, twiddles rounded from long
-// double on the host):
+// memory.  Grids with Ng = 32 * 2^p (64 <= Ng <= 1024) use warp-shuffle
+// transforms (one line per warp, in registers); every other 5-smooth even
+// grid uses a block-wide Stockham autosort (radices 8/4/2/3/5).  Twiddles
+// are rounded from long double on the host.
 //   pass I : tiles [all i] x [K columns of k] for one j.  Because k_y and k_z
 //            are constant along i, only two transforms are needed:
 //            A_x = FFT_i(S k_x), A_0 = FFT_i(S).
@@ -22,6 +24,7 @@
 // Traffic: S read once; 2 + 3 spectra written, 5 read; 3 real fields written.
 #include "ez_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -306,6 +309,263 @@ fft_pass_k(const cplx *__restrict__ s0, const cplx *__restrict__ s1,
   if ((threadIdx.x & 31) == 0) atomicMax(&stats->psimax_bits, __float_as_uint(mx));
 }
 
+// ===================================================== warp-shuffle FFTs ==
+//
+// Lines of length n = 32 E (E a power of two, E <= 32) are transformed by one
+// warp entirely in registers: lane l holds x[32 m + l] (m < E), does an
+// E-point DFT in registers, multiplies by exp(S 2 pi i l k / n), and the
+// 32-point DFTs across the lanes are done by five radix-2 decimation-in-
+// frequency stages with __shfl_xor_sync.  Lane l then holds X[k + E r(l)]
+// for k < E, r(l) = 5-bit reversal of l.  Tiles are staged in shared memory
+// column-major (one line per column, line stride n + 1) with the element
+// index XOR-swizzled by bits 4..7, which keeps both the strided line loads
+// and the bit-reversed stores (nearly) free of bank conflicts.
+
+__constant__ double2 c_w32[32];              // exp(+2 pi i k / 32)
+
+template <int S>
+__device__ __forceinline__ cplx w32(int k) {
+  const double2 w = c_w32[k & 31];
+  cplx r;
+  r.x = (rt) w.x;
+  r.y = (rt) (S * w.y);
+  return r;
+}
+
+template <int E, int S> struct RegDft;
+template <int S> struct RegDft<1, S> { __device__ static void run(cplx *) {} };
+template <int S> struct RegDft<2, S> { __device__ static void run(cplx *v) { dft2<S>(v); } };
+template <int S> struct RegDft<4, S> { __device__ static void run(cplx *v) { dft4<S>(v); } };
+template <int S> struct RegDft<8, S> { __device__ static void run(cplx *v) { dft8<S>(v); } };
+template <int E, int S> struct RegDft {
+  // radix-2 decimation in time from two half-size DFTs
+  __device__ static void run(cplx *v) {
+    cplx ev[E / 2], od[E / 2];
+#pragma unroll
+    for (int k = 0; k < E / 2; k++) { ev[k] = v[2 * k]; od[k] = v[2 * k + 1]; }
+    RegDft<E / 2, S>::run(ev);
+    RegDft<E / 2, S>::run(od);
+#pragma unroll
+    for (int k = 0; k < E / 2; k++) {
+      const cplx t = cmul(od[k], w32<S>(k * (32 / E)));
+      v[k] = cadd(ev[k], t);
+      v[k + E / 2] = csub(ev[k], t);
+    }
+  }
+};
+
+__device__ __forceinline__ int brev5(int l) { return __brev((unsigned) l) >> 27; }
+
+__device__ __forceinline__ cplx shfl_xor_c(cplx v, int m) {
+  cplx r;
+  r.x = __shfl_xor_sync(0xffffffffu, v.x, m);
+  r.y = __shfl_xor_sync(0xffffffffu, v.y, m);
+  return r;
+}
+
+// tw[e] = exp(+2 pi i e / n) in shared memory
+template <int E, int S>
+__device__ __forceinline__ void warp_fft(cplx *v, const cplx *tw, int lane) {
+  RegDft<E, S>::run(v);
+#pragma unroll
+  for (int k = 1; k < E; k++) {
+    cplx w = tw[lane * k];
+    if (S < 0) w.y = -w.y;
+    v[k] = cmul(v[k], w);
+  }
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    const cplx w = w32<S>((lane & (h - 1)) * (16 / h));
+    const bool hi = (lane & h) != 0;
+#pragma unroll
+    for (int k = 0; k < E; k++) {
+      const cplx b = shfl_xor_c(v[k], h);
+      v[k] = hi ? cmul(csub(b, v[k]), w) : cadd(v[k], b);
+    }
+  }
+}
+
+__device__ __forceinline__ int swz(int m) { return m ^ ((m >> 4) & 15); }
+
+constexpr int WNW = 8;                       // warps per block
+constexpr int WK = 8;                        // columns per tile (passes I, J)
+
+// pass I: A_x = FFT_i(S k_x), A_0 = FFT_i(S); one column per warp.
+template <int E>
+__global__ void __launch_bounds__(32 * WNW, 2)
+wpass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0,
+    int Ng, int Nkp, const cplx *__restrict__ twn) {
+  constexpr int n = 32 * E, LS = n + 1;
+  extern __shared__ unsigned char smraw[];
+  cplx *tw = (cplx *) smraw;
+  cplx *b0 = tw + n;                         // WK lines: S, then A_0
+  cplx *b1 = b0 + WK * LS;                   // WK lines: A_x
+  const int j = blockIdx.x, k0 = blockIdx.y * WK;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
+  const size_t pst = (size_t) Ng * Nkp;
+#pragma unroll 4
+  for (int e = threadIdx.x; e < n * WK; e += 32 * WNW) {
+    const int i = e / WK, c = e - i * WK;
+    b0[c * LS + swz(i)] = S[i * pst + (size_t) j * Nkp + k0 + c];
+  }
+  __syncthreads();
+  const int r = brev5(lane);
+  for (int c = w; c < WK; c += WNW) {
+    cplx v[E];
+#pragma unroll
+    for (int m = 0; m < E; m++) {
+      const int i = 32 * m + lane;
+      v[m] = b0[c * LS + swz(i)];
+      const rt f = freq_of(i, Ng);
+      v[m].x *= f;
+      v[m].y *= f;
+    }
+    warp_fft<E, 1>(v, tw, lane);
+#pragma unroll
+    for (int k = 0; k < E; k++) b1[c * LS + swz(k + E * r)] = v[k];
+#pragma unroll
+    for (int m = 0; m < E; m++) v[m] = b0[c * LS + swz(32 * m + lane)];
+    warp_fft<E, 1>(v, tw, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < E; k++) b0[c * LS + swz(k + E * r)] = v[k];
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (int e = threadIdx.x; e < n * WK; e += 32 * WNW) {
+    const int i = e / WK, c = e - i * WK;
+    const size_t g = i * pst + (size_t) j * Nkp + k0 + c;
+    Ax[g] = b1[c * LS + swz(i)];
+    A0[g] = b0[c * LS + swz(i)];
+  }
+}
+
+// pass J: B_x = FFT_j(A_x) -> s1, B_y = FFT_j(A_0 k_y) -> s0,
+// B_0 = FFT_j(A_0) -> s2.
+template <int E>
+__global__ void __launch_bounds__(32 * WNW, 2)
+wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
+    int Ng, int Nkp, const cplx *__restrict__ twn) {
+  constexpr int n = 32 * E, LS = n + 1;
+  extern __shared__ unsigned char smraw[];
+  cplx *tw = (cplx *) smraw;
+  cplx *bx = tw + n;                         // A_x -> B_x
+  cplx *b0 = bx + WK * LS;                   // A_0 -> B_0
+  cplx *by = b0 + WK * LS;                   // B_y
+  const int x = blockIdx.x, k0 = blockIdx.y * WK;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
+  const size_t base = (size_t) x * Ng * Nkp + k0;
+#pragma unroll 4
+  for (int e = threadIdx.x; e < n * WK; e += 32 * WNW) {
+    const int j = e / WK, c = e - j * WK;
+    const size_t g = base + (size_t) j * Nkp + c;
+    bx[c * LS + swz(j)] = s1[g];
+    b0[c * LS + swz(j)] = s2[g];
+  }
+  __syncthreads();
+  const int r = brev5(lane);
+  for (int c = w; c < WK; c += WNW) {
+    cplx v[E];
+#pragma unroll
+    for (int m = 0; m < E; m++) v[m] = bx[c * LS + swz(32 * m + lane)];
+    warp_fft<E, 1>(v, tw, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < E; k++) bx[c * LS + swz(k + E * r)] = v[k];
+#pragma unroll
+    for (int m = 0; m < E; m++) {
+      const int jj = 32 * m + lane;
+      v[m] = b0[c * LS + swz(jj)];
+      const rt f = freq_of(jj, Ng);
+      v[m].x *= f;
+      v[m].y *= f;
+    }
+    warp_fft<E, 1>(v, tw, lane);
+#pragma unroll
+    for (int k = 0; k < E; k++) by[c * LS + swz(k + E * r)] = v[k];
+#pragma unroll
+    for (int m = 0; m < E; m++) v[m] = b0[c * LS + swz(32 * m + lane)];
+    warp_fft<E, 1>(v, tw, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < E; k++) b0[c * LS + swz(k + E * r)] = v[k];
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (int e = threadIdx.x; e < n * WK; e += 32 * WNW) {
+    const int j = e / WK, c = e - j * WK;
+    const size_t g = base + (size_t) j * Nkp + c;
+    s1[g] = bx[c * LS + swz(j)];
+    s0[g] = by[c * LS + swz(j)];
+    s2[g] = b0[c * LS + swz(j)];
+  }
+}
+
+// pass K: per (x, y) row, c2r of B_x (s1), B_y (s0) and k B_0 (s2) through a
+// half-length complex FFT (n = Ng/2 = 32 E); one row per warp.
+template <int E>
+__global__ void __launch_bounds__(32 * WNW, 3)
+wpass_k(const cplx *__restrict__ s0, const cplx *__restrict__ s1,
+    const cplx *__restrict__ s2, real *__restrict__ p0, real *__restrict__ p1,
+    real *__restrict__ p2, int Ng, int Nkp, size_t nrows,
+    const cplx *__restrict__ twh, const cplx *__restrict__ twg,
+    EzCicStats *stats) {
+  constexpr int n = 32 * E, LS = n + 1;      // n = Ng / 2
+  extern __shared__ unsigned char smraw[];
+  cplx *tw = (cplx *) smraw;                 // n: exp(+2 pi i e / n)
+  cplx *tg = tw + n;                         // n: exp(+2 pi i k / Ng)
+  cplx *st = tg + n;                         // WNW staging lines
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) { tw[e] = twh[e]; tg[e] = twg[e]; }
+  __syncthreads();
+  cplx *sl = st + w * LS;
+  float mx = 0.f;
+  for (size_t row = (size_t) blockIdx.x * WNW + w; row < nrows;
+       row += (size_t) gridDim.x * WNW) {
+#pragma unroll 1
+    for (int comp = 0; comp < 3; comp++) {
+      const cplx *X = ((comp == 0) ? s1 : (comp == 1) ? s0 : s2) + row * Nkp;
+      real *dst = ((comp == 0) ? p0 : (comp == 1) ? p1 : p2) + row * Ng;
+      cplx v[E];
+#pragma unroll
+      for (int m = 0; m < E; m++) {
+        const int k = 32 * m + lane;
+        cplx a = X[k], b = X[n - k];
+        if (comp == 2) {
+          a.x *= (rt) k; a.y *= (rt) k;
+          b.x *= (rt) (n - k); b.y *= (rt) (n - k);
+        }
+        const rt xr = a.x, xi = (k == 0) ? (rt) 0 : a.y;
+        const rt yr = b.x, yi = (k == 0) ? (rt) 0 : -b.y;
+        const rt er = xr + yr, ei = xi + yi;
+        const rt dr = xr - yr, di = xi - yi;
+        const cplx t = tg[k];
+        const rt orr = dr * t.x - di * t.y, oi = dr * t.y + di * t.x;
+        v[m].x = er - oi;
+        v[m].y = ei + orr;
+      }
+      warp_fft<E, 1>(v, tw, lane);
+      const int r = brev5(lane);
+#pragma unroll
+      for (int k = 0; k < E; k++) sl[swz(k + E * r)] = v[k];
+      __syncwarp();
+      cplx *d2 = (cplx *) dst;
+#pragma unroll
+      for (int m = 0; m < E; m++) {
+        const cplx z = sl[swz(32 * m + lane)];
+        d2[32 * m + lane] = z;
+        mx = fmaxf(mx, fmaxf(fabsf((float) z.x), fabsf((float) z.y)));
+      }
+      __syncwarp();
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) atomicMax(&stats->psimax_bits, __float_as_uint(mx));
+}
+
 // ------------------------------------------- forward transforms (r2c) ---
 // Row r2c along k (sign -1): even/odd packing into a half-length complex FFT,
 // then X[k] = E[k] + exp(-2 pi i k/Ng) O[k] for k = 0..Ng/2.
@@ -451,8 +711,101 @@ bool ez_fft_supported(int Ng) {
   return sm_j <= 200 * 1024 && sm_k <= 200 * 1024;
 }
 
+namespace {
+bool w32_ready[64] = {false};
+
+bool set_w32(int dev) {
+  if (dev < 0 || dev >= 64) return false;
+  if (w32_ready[dev]) return true;
+  double2 h[32];
+  const long double tpi = 6.283185307179586476925286766559005768L;
+  for (int k = 0; k < 32; k++) {
+    h[k].x = (double) cosl(tpi * k / 32);
+    h[k].y = (double) sinl(tpi * k / 32);
+  }
+  if (!EZ_CUDA_OK(cudaMemcpyToSymbol(c_w32, h, sizeof(h)))) return false;
+  w32_ready[dev] = true;
+  return true;
+}
+
+// E = n / 32 when n is 32 times a power of two up to 32, else 0.
+int warp_e(int n) {
+  if (n % 32) return 0;
+  const int e = n / 32;
+  return (e <= 32 && (e & (e - 1)) == 0) ? e : 0;
+}
+
+// The warp-shuffle passes serve Ng when Ng and Ng/2 are both 32 E and the
+// pass-J tile (three lines of WK columns) fits the 227 KB per-block limit.
+bool warp_path(int Ng) {
+  if (!warp_e(Ng) || !warp_e(Ng / 2)) return false;
+  return sizeof(cplx) * ((size_t) Ng + 3 * WK * (size_t) (Ng + 1)) <= 227 * 1024;
+}
+
+template <int E>
+int run_wpass_ij(EzMesh *m, const FftPlanDev &pn) {
+  const int Ng = m->Ng;
+  const size_t n = 32 * E, LS = n + 1;
+  const size_t sm_i = sizeof(cplx) * (n + 2 * WK * LS);
+  const size_t sm_j = sizeof(cplx) * (n + 3 * WK * LS);
+  cudaFuncSetAttribute(wpass_i<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_i);
+  cudaFuncSetAttribute(wpass_j<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_j);
+  const int nkt = (m->Nk + WK - 1) / WK;
+  ez_stage_begin(m, ST_FFT_I);
+  wpass_i<E><<<dim3(Ng, nkt), 32 * WNW, sm_i, m->stream>>>(m->spec[0], m->spec[1],
+      m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
+  ez_stage_end(m, ST_FFT_I);
+  ez_stage_begin(m, ST_FFT_J);
+  wpass_j<E><<<dim3(Ng, nkt), 32 * WNW, sm_j, m->stream>>>(m->spec[0], m->spec[1],
+      m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
+  ez_stage_end(m, ST_FFT_J);
+  return 0;
+}
+
+template <int E>
+int run_wpass_k(EzMesh *m, const FftPlanDev &ph, const cplx *twg) {
+  const int Ng = m->Ng;
+  const size_t n = 32 * E;
+  const size_t sm = sizeof(cplx) * (2 * n + WNW * (n + 1));
+  cudaFuncSetAttribute(wpass_k<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+  const size_t nrows = (size_t) Ng * Ng;
+  const unsigned nb = (unsigned) std::min<size_t>((nrows + WNW - 1) / WNW, 148 * 16);
+  ez_stage_begin(m, ST_FFT_K);
+  wpass_k<E><<<nb, 32 * WNW, sm, m->stream>>>(m->spec[0], m->spec[1], m->spec[2],
+      m->psi[0], m->psi[1], m->psi[2], Ng, m->Nkp, nrows, ph.tw, twg,
+      (EzCicStats *) m->stats); ez_count_launch();
+  ez_stage_end(m, ST_FFT_K);
+  return 0;
+}
+}  // namespace
+
 int ez_fft_c2r_psi(EzMesh *m) {
   const int Ng = m->Ng, Nkp = m->Nkp, Nh = Ng / 2;
+  const int Ei = warp_e(Ng), Ek = warp_e(Nh);
+  if (warp_path(Ng) && m->Nkp % WK == 0 && set_w32(m->device)) {
+    FftPlanDev pn, ph;
+    if (!make_plan(m->device, Ng, &pn) || !make_plan(m->device, Nh, &ph))
+      return EZMOCK_ERR_UNKNOWN;
+    const cplx *twg = twiddles(m->device, Ng);
+    if (!twg) return EZMOCK_ERR_UNKNOWN;
+    switch (Ei) {
+      case 2: run_wpass_ij<2>(m, pn); break;
+      case 4: run_wpass_ij<4>(m, pn); break;
+      case 8: run_wpass_ij<8>(m, pn); break;
+      case 16: run_wpass_ij<16>(m, pn); break;
+      default: run_wpass_ij<32>(m, pn); break;
+    }
+    cudaMemsetAsync(&((EzCicStats *) m->stats)->psimax_bits, 0, sizeof(unsigned int), m->stream);
+    switch (Ek) {
+      case 1: run_wpass_k<1>(m, ph, twg); break;
+      case 2: run_wpass_k<2>(m, ph, twg); break;
+      case 4: run_wpass_k<4>(m, ph, twg); break;
+      case 8: run_wpass_k<8>(m, ph, twg); break;
+      default: run_wpass_k<16>(m, ph, twg); break;
+    }
+    m->psimax_valid = true;
+    return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+  }
   const int K = ez_fft_tile_k(Ng);
   FftPlanDev pn, ph;
   if (!make_plan(m->device, Ng, &pn) || !make_plan(m->device, Nh, &ph))

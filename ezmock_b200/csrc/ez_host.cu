@@ -8,8 +8,10 @@
 #include "ez_internal.cuh"
 #include "ezmock_b200.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <thread>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -149,6 +151,7 @@ void mesh_free_device(EzMesh *m) {
   if (m->stats) cudaFree(m->stats);
   if (m->cat) cudaFree(m->cat);
   if (m->h_stage) cudaFreeHost(m->h_stage);
+  for (int i = 0; i < 2; i++) if (m->d2h_ev[i]) cudaEventDestroy(m->d2h_ev[i]);
   if (m->stream) cudaStreamDestroy(m->stream);
   for (int i = 0; i < 2 * ST_NSTAGE; i++) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
   for (int i = 0; i < 8; i++) if (m->mark[i]) cudaEventDestroy(m->mark[i]);
@@ -571,26 +574,70 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
       return (*err = EZMOCK_ERR_MEMORY);
     }
   }
-  // device -> pinned staging -> caller's malloc() arrays
-  const size_t bytes = 6 * n * sizeof(real);
+  // device -> pinned staging (two 8 MB halves, DMA of one overlapping the
+  // copy-out of the other) -> the caller's malloc() arrays, copied out by
+  // several host threads
   ez_stage_begin(m, ST_D2H);
-  if (bytes > m->h_stage_cap) {
+  const size_t half = (size_t) 8 << 20;
+  if (m->h_stage_cap < 2 * half) {
     if (m->h_stage) cudaFreeHost(m->h_stage);
     m->h_stage = nullptr;
     m->h_stage_cap = 0;
-    if (!EZ_CUDA_OK(cudaMallocHost(&m->h_stage, bytes))) {
+    if (!EZ_CUDA_OK(cudaMallocHost(&m->h_stage, 2 * half))) {
       for (int j = 0; j < 6; j++) free(cat[j]);
       return (*err = EZMOCK_ERR_MEMORY);
     }
-    m->h_stage_cap = bytes;
+    m->h_stage_cap = 2 * half;
   }
-  if (!EZ_CUDA_OK(cudaMemcpyAsync(m->h_stage, m->cat, bytes, cudaMemcpyDeviceToHost, m->stream)) ||
-      !EZ_CUDA_OK(cudaStreamSynchronize(m->stream))) {
+  if (!m->d2h_ev[0]) {
+    cudaEventCreateWithFlags(&m->d2h_ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&m->d2h_ev[1], cudaEventDisableTiming);
+  }
+  int nthr = CONF(ez)->nthread > 0 ? CONF(ez)->nthread : (int) std::thread::hardware_concurrency();
+  nthr = std::max(1, std::min(nthr, 8));
+  const size_t bytes_arr = n * sizeof(real);
+  const size_t per = half / sizeof(real);               // reals per half
+  struct Piece { int arr; size_t off, len; };
+  std::vector<Piece> pieces;
+  for (int a = 0; a < 6; a++)
+    for (size_t o = 0; o < n; o += per) pieces.push_back({a, o, std::min(per, n - o)});
+  bool ok = true;
+  auto issue = [&](size_t k) {
+    const Piece &pc = pieces[k];
+    real *stage = (real *) ((char *) m->h_stage + (k & 1) * half);
+    ok = ok && EZ_CUDA_OK(cudaMemcpyAsync(stage, m->cat + (size_t) pc.arr * n + pc.off,
+        pc.len * sizeof(real), cudaMemcpyDeviceToHost, m->stream));
+    ok = ok && EZ_CUDA_OK(cudaEventRecord(m->d2h_ev[k & 1], m->stream));
+  };
+  if (!pieces.empty()) issue(0);
+  for (size_t k = 0; k < pieces.size() && ok; k++) {
+    if (k + 1 < pieces.size()) {
+      // the other half is free once its previous copy-out has finished
+      issue(k + 1);
+    }
+    ok = ok && EZ_CUDA_OK(cudaEventSynchronize(m->d2h_ev[k & 1]));
+    const Piece &pc = pieces[k];
+    const char *src = (const char *) m->h_stage + (k & 1) * half;
+    char *dst = (char *) (cat[pc.arr] + pc.off);
+    const size_t nb = pc.len * sizeof(real);
+    const int nt = (nb >= ((size_t) 1 << 20)) ? nthr : 1;
+    if (nt == 1) memcpy(dst, src, nb);
+    else {
+      std::vector<std::thread> th;
+      const size_t step = (nb + nt - 1) / nt;
+      for (int t = 0; t < nt; t++) {
+        const size_t b0 = std::min(nb, t * step), b1 = std::min(nb, b0 + step);
+        if (b1 > b0) th.emplace_back([=]() { memcpy(dst + b0, src + b0, b1 - b0); });
+      }
+      for (auto &x : th) x.join();
+    }
+  }
+  (void) bytes_arr;
+  if (!ok) {
     for (int j = 0; j < 6; j++) free(cat[j]);
     return (*err = EZMOCK_ERR_UNKNOWN);
   }
   ez_stage_end(m, ST_D2H);
-  for (int i = 0; i < 6; i++) memcpy(cat[i], m->h_stage + i * n, n * sizeof(real));
   *ntracer = n;
   *x = cat[0]; *y = cat[1]; *z = cat[2];
   *vx = cat[3]; *vy = cat[4]; *vz = cat[5];

@@ -109,6 +109,7 @@ struct EzMesh {
   size_t cat_n;            // length of the last catalogue (array stride)
   real *h_stage;           // pinned host staging for the catalogue
   size_t h_stage_cap;
+  cudaEvent_t d2h_ev[2];   // staging halves ready
 };
 
 // Device-side statistics of the displacement/density assignment.
