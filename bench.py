@@ -82,12 +82,13 @@ def read_peak():
         return 6650.0, "fallback"
 
 
-def read_traffic():
-    """Per-launch DRAM bytes of each kernel from the committed ncu summary."""
+def read_traffic(workload):
+    """Per-launch DRAM bytes of each stage's kernel for `workload`, from the
+    committed ncu summary (profiles/traffic.json)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
-            return json.load(f)
+            return json.load(f).get(workload, {})
     except Exception:
         return {}
 
@@ -320,7 +321,7 @@ def main():
                   for s in med}
     dom = max((s for s in algo if s in med), key=lambda s: med[s])
     achieved = algo[dom] / (med[dom] * 1e-3) / 1e9
-    traffic = read_traffic().get(dom)
+    traffic = read_traffic(cfg.name).get(dom)
     roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "algorithmic_bytes": algo[dom]}

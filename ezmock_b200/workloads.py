@@ -79,6 +79,9 @@ CONFIGS = {
     "plain128": MockConfig("plain128", 128, 1000.0, 1, 3e-4, 0.6, 15.0, 0.35, 300.0),
     # Single mock at 512^3, box 2500 Mpc/h (the bench workload).
     "single512": MockConfig("single512", 512, 2500.0, 1, 2e-4, 0.8, 20.0, 0.3, 400.0),
+    # The 512^3 mock at half the size and box (same cell size and tracer
+    # density): the profiling case, fields still larger than the 126 MB L2.
+    "single256": MockConfig("single256", 256, 1250.0, 1, 2e-4, 0.8, 20.0, 0.3, 400.0),
     # 1024^3, box 5000 Mpc/h, one field populated three times.
     "multi1024": MockConfig(
         "multi1024", 1024, 5000.0, 1, 2e-4, 0.5, 10.0, 0.3, 250.0,
