@@ -78,6 +78,9 @@ def load(prec=32):
     L.EZmockB200_rng_raw.restype = ctypes.c_int
     L.EZmockB200_rng_raw.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
                                      ctypes.c_uint64, _vp]
+    L.EZmockB200_mt19937_fill_noalloc.restype = ctypes.c_int
+    L.EZmockB200_mt19937_fill_noalloc.argtypes = [ctypes.c_uint64, ctypes.c_uint64,
+                                                  ctypes.c_uint64, _vp, _vp]
     L.EZmockB200_sync.restype = ctypes.c_int
     L.EZmockB200_sync.argtypes = [_vp]
     L.EZmockB200_real_size.restype = ctypes.c_int

@@ -792,6 +792,8 @@ const char *EZmock_errmsg(const int err) {
     case EZMOCK_ERR_FFT_INIT:   return "failed to initialise FFTW with OpenMP";
     case EZMOCK_ERR_FILE:       return "failed to write to the output file";
     case EZMOCK_ERR_UNKNOWN:    return "unknown error";
+    case EZMOCKB200_ERR_SCRATCH_SIZE:
+      return "draw count exceeds the static scratch of the no-allocation fill";
     default:                    return "unregistered error code";
   }
 }

@@ -23,6 +23,7 @@
 //    level jumping all known chunk states by 2^m * L in parallel.  Each chunk
 //    is then generated by one block with the three-phase twist.
 #include "ez_internal.cuh"
+#include "ezmock_b200.h"
 
 #include <algorithm>
 #include <cstdlib>
@@ -632,4 +633,149 @@ int ez_rng_fill_prepared(EzMesh *m, int ran, uint64_t seed, int i,
   r.p = m->rng_prep[i].p;
   r.first = m->rng_prep[i].first;
   return mt_generate(m, r, count, out);
+}
+
+// ============================================================================
+//            MT19937 fill with static device scratch (no allocation)
+// ============================================================================
+//
+// Same kernels and stream as ez_rng_fill (MT19937), but the chunk states, the
+// jump descriptors and the jump polynomials live in file-scope device arrays
+// instead of memory obtained from cudaMalloc.  It serves callers that must
+// not allocate device memory on this path: a host framework that owns the
+// whole device memory through its own pool (a caching allocator that a
+// cudaMalloc would fight for memory), and pipelines where a cudaMalloc/
+// cudaFree pair would add an implicit device synchronisation between
+// otherwise asynchronous launches.
+//
+// Limits: one fill has at most NA_MAXCHUNK = 128 chunks of at most 2^40 draws,
+// so count <= 2^47; each chunk needs one 624-word state, plus the seed state.
+// Scratch: 129 x 624 words of states, 128 jump descriptors, 72 polynomial
+// indices (324,320 bytes).  Nothing in it has to start at zero: every word a
+// kernel reads was written earlier in the same call.  The jump table
+// x^(2^k) mod phi (64 x 312 words, 159,744 bytes) is copied into its own
+// static array by the first call on each device.
+//
+// The scratch is one per device: calls that overlap on the same device (two
+// streams, or two host threads) race on it and must be serialised by the
+// caller.
+namespace {
+
+constexpr int NA_MAXCHUNK = 128;
+constexpr int NA_STATES = 1 + NA_MAXCHUNK;
+constexpr int NA_MAXDESC = NA_MAXCHUNK;          // 1 + (1 + 2 + ... + 64)
+constexpr int NA_MAXPOLY = 64 + 8;               // bits of start + doublings
+constexpr size_t NA_DESC_OFF = (size_t) NA_STATES * MT_N;        // words
+constexpr size_t NA_PLIST_OFF = NA_DESC_OFF + 4 * NA_MAXDESC;
+constexpr size_t NA_WORDS = NA_PLIST_OFF + NA_MAXPOLY;
+static_assert(NA_DESC_OFF % 4 == 0, "descriptors must be 16-byte aligned");
+
+__device__ __align__(256) uint32_t na_scratch[NA_WORDS];
+__device__ __align__(256) uint64_t na_xpow[64 * MT_PW];
+
+struct NaSeed {
+  uint32_t w[MT_N];                              // seed window (2,496 bytes)
+  uint64_t start;
+  int l, p;
+};
+
+// Writes the seed window into state 0 and builds the descriptors of the
+// jump to `start` (level 0, polynomials = set bits of start) and of the
+// doubling levels (level m + 1: 2^m jumps by 2^(l + m) draws), in the
+// layout mt_prepare_ranges uses for a single range.
+__global__ void na_plan_kernel(uint32_t *scratch, NaSeed s) {
+  uint32_t *states = scratch;
+  int4 *desc = (int4 *) (scratch + NA_DESC_OFF);
+  int *plist = (int *) (scratch + NA_PLIST_OFF);
+  for (int k = threadIdx.x; k < MT_N; k += blockDim.x) states[k] = s.w[k];
+  if (threadIdx.x == 0) {
+    int np = 0;
+    for (int k = 0; k < 64; k++)
+      if ((s.start >> k) & 1ULL) plist[np++] = k;
+    desc[0] = make_int4(0, 1, 0, np);
+    for (int lev = 0; lev < s.p; lev++) {
+      plist[np] = s.l + lev;
+      for (int t = 0; t < (1 << lev); t++)
+        desc[(1 << lev) + t] = make_int4(1 + t, 1 + t + (1 << lev), np, 1);
+      np++;
+    }
+  }
+}
+
+struct NaDevice {
+  bool ready = false;
+  uint32_t *scratch = nullptr;
+  uint64_t *xpow = nullptr;
+};
+std::mutex g_na_mu;
+NaDevice g_na[64];
+
+// One-time set-up for the current device: host jump tables (shared with the
+// allocating path), device addresses of the static arrays, the table copy,
+// and the Horner kernel's shared-memory limit.  Synchronous.
+int na_setup(int dev, NaDevice **out) {
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  if (dev < 0 || dev >= 64) return EZMOCK_ERR_UNKNOWN;
+  NaDevice &d = g_na[dev];
+  if (!d.ready) {
+    {
+      std::lock_guard<std::mutex> lt(g_mt_mu);
+      if (!g_mt_built) { build_mt_tables(g_mt); g_mt_built = true; }
+    }
+    if (!g_mt.ok || g_mt.xpow.size() != (size_t) 64 * MT_PW) return EZMOCK_ERR_RNG_SET;
+    void *ps = nullptr, *px = nullptr;
+    if (!EZ_CUDA_OK(cudaGetSymbolAddress(&ps, na_scratch)) ||
+        !EZ_CUDA_OK(cudaGetSymbolAddress(&px, na_xpow)) || !ps || !px) {
+      cudaGetLastError();
+      return EZMOCK_ERR_UNKNOWN;
+    }
+    if (!EZ_CUDA_OK(cudaMemcpy(px, g_mt.xpow.data(), g_mt.xpow.size() * sizeof(uint64_t),
+            cudaMemcpyHostToDevice)) ||
+        !EZ_CUDA_OK(cudaFuncSetAttribute(mt_horner_kernel,
+            cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int) ((HG * HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t)))))
+      return EZMOCK_ERR_UNKNOWN;
+    d.scratch = (uint32_t *) ps;
+    d.xpow = (uint64_t *) px;
+    d.ready = true;
+  }
+  *out = &d;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int EZmockB200_mt19937_fill_noalloc(const uint64_t seed,
+    const uint64_t start, const uint64_t count, uint32_t *d_out, void *stream) {
+  if (!count) return 0;
+  if (!d_out) return EZMOCK_ERR_ARG_NULL;
+  if (count > EZMOCKB200_NOALLOC_MAX_DRAWS || start > UINT64_MAX - count)
+    return EZMOCKB200_ERR_SCRATCH_SIZE;
+  const MtRange r = mt_plan(start, count);
+  if (r.p > 7 || ((uint64_t) 1 << (r.l + r.p)) < count) return EZMOCKB200_ERR_SCRATCH_SIZE;
+  int dev = -1;
+  if (!EZ_CUDA_OK(cudaGetDevice(&dev))) { cudaGetLastError(); return EZMOCK_ERR_UNKNOWN; }
+  NaDevice *d = nullptr;
+  int e = na_setup(dev, &d);
+  if (e) return e;
+  cudaStream_t st = (cudaStream_t) stream;
+  NaSeed s;
+  mt_seed_window(seed, s.w);
+  s.start = start;
+  s.l = r.l;
+  s.p = r.p;
+  na_plan_kernel<<<1, 256, 0, st>>>(d->scratch, s); ez_count_launch();
+  const int4 *desc = (const int4 *) (d->scratch + NA_DESC_OFF);
+  const int *plist = (const int *) (d->scratch + NA_PLIST_OFF);
+  const size_t smem = (HG * HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t);
+  mt_horner_kernel<<<1, H_THREADS, smem, st>>>(d->scratch, desc, d->xpow, plist);
+  ez_count_launch();
+  for (int lev = 0; lev < r.p; lev++) {
+    mt_horner_kernel<<<1 << lev, H_THREADS, smem, st>>>(d->scratch, desc + (1 << lev),
+        d->xpow, plist); ez_count_launch();
+  }
+  const uint64_t L = 1ULL << r.l;
+  mt_gen_kernel<<<(unsigned) ((count + L - 1) / L), G_THREADS, 0, st>>>(
+      d->scratch + MT_N, L, count, d_out); ez_count_launch();
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }

@@ -57,6 +57,31 @@ int EZmockB200_select_counts(EZMOCK *ez, const real *rhot,
 int EZmockB200_rng_raw(const int randgen, const uint64_t seed,
     const uint64_t start, const uint64_t count, uint32_t *out);
 
+/* MT19937 draws [start, start+count) of stream `seed` (the stream of
+   EZmockB200_rng_raw with randgen 1) written to the DEVICE buffer `d_out`
+   (count uint32 values) on CUDA stream `stream` (a cudaStream_t; NULL for
+   the legacy default stream), without allocating memory.  No counterpart in
+   the reference: it is for callers that cannot allocate device memory on
+   this path (a framework that owns the device memory through its own pool,
+   or a pipeline that must not take the implicit synchronisation of
+   cudaMalloc/cudaFree).  Scratch is a static device array of 324,320 bytes
+   per device (129 generator states of 624 words, 128 jump descriptors, 72
+   polynomial indices), which bounds one call to count <=
+   EZMOCKB200_NOALLOC_MAX_DRAWS; larger counts (or start + count beyond
+   2^64) return EZMOCKB200_ERR_SCRATCH_SIZE without launching anything.
+   The scratch needs no zeroing.  The first call on a device (the device
+   current at the call) does a synchronous set-up: the host jump tables
+   (built once per process), the device addresses of the static arrays, a
+   copy of the 159,744-byte jump table; make that first call before any
+   stream capture.  Later calls only launch kernels on `stream` and return
+   without waiting.  There is one scratch per device: calls that overlap on
+   the same device race on it, so the caller serialises them (one stream,
+   one host thread at a time). */
+#define EZMOCKB200_NOALLOC_MAX_DRAWS ((uint64_t) 1 << 47)
+#define EZMOCKB200_ERR_SCRATCH_SIZE 64
+int EZmockB200_mt19937_fill_noalloc(const uint64_t seed, const uint64_t start,
+    const uint64_t count, uint32_t *d_out, void *stream);
+
 /* Waits for all work of the instance. */
 int EZmockB200_sync(EZMOCK *ez);
 
