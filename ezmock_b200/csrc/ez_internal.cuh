@@ -98,7 +98,7 @@ struct EzMesh {
   size_t scratch_cap;
   void *rng_scratch;       // skip-ahead states of the MT19937 streams
   size_t rng_scratch_cap;
-  struct { uint64_t start, cap; int l, p; size_t first; } rng_prep[4];
+  struct { uint64_t start, cap; int l, P; size_t first; } rng_prep[4];  // P chunks of 2^l
   int rng_nprep;           // prepared stream ranges (ez_rng_prepare)
   size_t rng_prep_end;     // first free state slot after them
   unsigned long long *fixacc;   // deterministic CIC accumulators (4 x N)

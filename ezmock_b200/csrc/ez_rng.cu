@@ -18,17 +18,24 @@
 //    Berlekamp-Massey and the table x^(2^k) mod phi by repeated squaring.  On
 //    the GPU one block applies p(T) with Horner's rule over 16-bit windows
 //    (four 16-entry tables of combinations of T^j s held in shared memory,
-//    one barrier per window).  Chunk states for a range [start, start + P*L) are
-//    built by one jump to `start` followed by log2(P) doubling levels, each
-//    level jumping all known chunk states by 2^m * L in parallel.  Each chunk
-//    is then generated by one block with the three-phase twist.
+//    one barrier per window).  Chunk c of a range [start, start + P*L) is
+//    reached directly from the seed window with x^(start + c L) mod phi; the
+//    host computes these polynomials once per (start, L) with carry-less
+//    products (ez_gf2.cpp) and keeps them on the device, so all P chunk
+//    states come from one launch.  Each chunk is then generated by one block
+//    through a ring buffer, 227 words per barrier.  (Without the host
+//    arithmetic the states are built by one jump to `start` and log2(P)
+//    doubling levels, the scheme the allocation-free entry point uses.)
 #include "ez_internal.cuh"
 #include "ezmock_b200.h"
+#include "ez_gf2.h"
 
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace {
@@ -227,71 +234,131 @@ __device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
   return y;
 }
 
+// Shared-memory layout of a Horner block: HG x HTAB x MT_N table words, the
+// window extended by HW words, two MT_N result buffers, one polynomial.
+constexpr size_t H_SMEM_WORDS = (size_t) HG * HTAB * MT_N + 3 * MT_N + HW;
+constexpr size_t H_SMEM = H_SMEM_WORDS * sizeof(uint32_t);
+constexpr size_t HJ_SMEM = (H_SMEM_WORDS + (H_SMEM_WORDS & 1)) * sizeof(uint32_t) +
+    MT_PW * sizeof(uint64_t);
+
+// Applies p(T) to the window held in ext[0, MT_N) (logical order), in place.
+// Horner's rule runs over 16-bit windows of p: r <- T^16 r + sum_g
+// tab_g[c_g], where tab_g[c] = sum_{j<4} c_j T^(4g+j) s are four 16-entry
+// tables of combinations of the source state, so each window costs one
+// barrier.  All threads of the block take part.
+__device__ __forceinline__ void horner_apply(uint32_t *ext, uint32_t *tab,
+    uint32_t *ra, uint32_t *rb, const uint64_t *p) {
+  const int t = threadIdx.x;
+  if (t < HW) ext[MT_N + t] = mt_f(ext[t], ext[t + 1], ext[MT_M + t]);
+  __syncthreads();
+  for (int e = t; e < HG * HTAB * MT_N; e += blockDim.x) {
+    const int gc = e / MT_N, k = e - gc * MT_N;
+    const int g = gc / HTAB, c = gc - g * HTAB;
+    uint32_t v = 0;
+#pragma unroll
+    for (int j = 0; j < HSUB; j++)
+      if (c & (1 << j)) v ^= ext[k + HSUB * g + j];
+    tab[e] = v;
+  }
+  for (int k = t; k < MT_N; k += blockDim.x) ra[k] = 0;
+  __syncthreads();
+  uint32_t *r0 = ra, *r1 = rb;
+  const int nwin = (MT_DEG + HW - 1) / HW;
+  for (int q = nwin - 1; q >= 0; q--) {
+    const int b = q * HW;                      // HW = 16 divides 64
+    const uint32_t bits = (uint32_t) (p[b >> 6] >> (b & 63)) & 0xffffu;
+    if (t < MT_N) {
+      uint32_t v;
+      if (t < MT_N - HW) v = r0[t + HW];
+      else {
+        const int s = t - (MT_N - HW);
+        v = mt_f(r0[s], r0[s + 1], r0[MT_M + s]);
+      }
+#pragma unroll
+      for (int g = 0; g < HG; g++)
+        v ^= tab[(g * HTAB + ((bits >> (HSUB * g)) & (HTAB - 1))) * MT_N + t];
+      r1[t] = v;
+    }
+    __syncthreads();
+    uint32_t *tmp = r0; r0 = r1; r1 = tmp;
+  }
+  for (int k = t; k < MT_N; k += blockDim.x) ext[k] = r0[k];
+  __syncthreads();
+}
+
 // Apply p(T) for each polynomial in `plist` (npoly entries, each MT_PW words
 // in `polys`) to state in[in_base + blockIdx.x]; result to out[out_base + b].
-// States are 624-word windows in logical order.  Horner's rule runs over
-// 16-bit windows of p: r <- T^16 r + sum_g tab_g[c_g], where tab_g[c] =
-// sum_{j<4} c_j T^(4g+j) s are four 16-entry tables of combinations of the
-// source state (shared memory), so each window costs one barrier.
-// Block b applies desc[b] = {in state, out state, first poly, npoly}.
+// States are 624-word windows in logical order.  Block b applies desc[b] =
+// {in state, out state, first poly, npoly}.
 __global__ void __launch_bounds__(H_THREADS)
 mt_horner_kernel(uint32_t *states, const int4 *__restrict__ desc,
     const uint64_t *__restrict__ polys, const int *__restrict__ plist_all) {
   extern __shared__ uint32_t sm[];
   const int4 dsc = desc[blockIdx.x];
-  const size_t in_base = (size_t) dsc.x, out_base = (size_t) dsc.y;
   const int *plist = plist_all + dsc.z;
-  const int npoly = dsc.w;
-  const uint32_t *states_in = states;
-  uint32_t *states_out = states;
   uint32_t *tab = sm;                        // HG x HTAB x MT_N
   uint32_t *ext = tab + HG * HTAB * MT_N;    // MT_N + HW
   uint32_t *ra = ext + MT_N + HW;            // MT_N
   uint32_t *rb = ra + MT_N;                  // MT_N
   const int t = threadIdx.x;
-  const uint32_t *src = states_in + in_base * MT_N;
+  const uint32_t *src = states + (size_t) dsc.x * MT_N;
   for (int k = t; k < MT_N; k += blockDim.x) ext[k] = src[k];
   __syncthreads();
-  for (int ip = 0; ip < npoly; ip++) {
-    const uint64_t *p = polys + (size_t) plist[ip] * MT_PW;
-    if (t < HW) ext[MT_N + t] = mt_f(ext[t], ext[t + 1], ext[MT_M + t]);
-    __syncthreads();
-    for (int e = t; e < HG * HTAB * MT_N; e += blockDim.x) {
-      const int gc = e / MT_N, k = e - gc * MT_N;
-      const int g = gc / HTAB, c = gc - g * HTAB;
-      uint32_t v = 0;
-#pragma unroll
-      for (int j = 0; j < HSUB; j++)
-        if (c & (1 << j)) v ^= ext[k + HSUB * g + j];
-      tab[e] = v;
+  for (int ip = 0; ip < dsc.w; ip++)
+    horner_apply(ext, tab, ra, rb, polys + (size_t) plist[ip] * MT_PW);
+  uint32_t *dst = states + (size_t) dsc.y * MT_N;
+  for (int k = t; k < MT_N; k += blockDim.x) dst[k] = ext[k];
+}
+
+// One direct jump per block: states[job.out] = job.poly(T) states[job.in].
+struct MtJob {
+  uint32_t in, out;
+  const uint64_t *poly;                      // MT_PW words, x^J mod phi
+};
+
+__global__ void __launch_bounds__(H_THREADS)
+mt_jump_kernel(uint32_t *states, const MtJob *__restrict__ jobs) {
+  extern __shared__ uint32_t sm[];
+  const MtJob job = jobs[blockIdx.x];
+  uint32_t *tab = sm;
+  uint32_t *ext = tab + HG * HTAB * MT_N;
+  uint32_t *ra = ext + MT_N + HW;
+  uint32_t *rb = ra + MT_N;
+  uint64_t *pp = (uint64_t *) (sm + H_SMEM_WORDS + (H_SMEM_WORDS & 1));
+  const int t = threadIdx.x;
+  const uint32_t *src = states + (size_t) job.in * MT_N;
+  for (int k = t; k < MT_N; k += blockDim.x) ext[k] = src[k];
+  for (int k = t; k < MT_PW; k += blockDim.x) pp[k] = job.poly[k];
+  __syncthreads();
+  horner_apply(ext, tab, ra, rb, pp);
+  uint32_t *dst = states + (size_t) job.out * MT_N;
+  for (int k = t; k < MT_N; k += blockDim.x) dst[k] = ext[k];
+}
+
+// Block c generates draws [c*L, min((c+1)*L, count)) from window states[c]
+// through a 1024-word ring: step g computes the 227 words 624+g .. 850+g,
+// which depend only on words g .. 623+g, so one barrier per step suffices.
+constexpr int R_THREADS = 256;
+__global__ void __launch_bounds__(R_THREADS)
+mt_ring_kernel(const uint32_t *__restrict__ states, uint64_t L, uint64_t count,
+    uint32_t *__restrict__ out) {
+  __shared__ uint32_t ring[1024];
+  const int t = threadIdx.x;
+  const uint64_t c0 = (uint64_t) blockIdx.x * L;
+  if (c0 >= count) return;
+  const uint64_t n = (count - c0 < L) ? count - c0 : L;
+  for (int k = t; k < MT_N; k += R_THREADS) ring[k] = states[(size_t) blockIdx.x * MT_N + k];
+  __syncthreads();
+  uint32_t *o = out + c0;
+  for (uint64_t g = 0; g < n; g += MT_N - MT_M) {
+    if (t < MT_N - MT_M && g + t < n) {
+      const uint32_t b = (uint32_t) g + t;   // logical index mod 2^32; 1024 | 2^32
+      const uint32_t y = mt_f(ring[b & 1023], ring[(b + 1) & 1023], ring[(b + MT_M) & 1023]);
+      ring[(b + MT_N) & 1023] = y;
+      o[g + t] = mt_temper(y);
     }
-    for (int k = t; k < MT_N; k += blockDim.x) ra[k] = 0;
-    __syncthreads();
-    uint32_t *r0 = ra, *r1 = rb;
-    const int nwin = (MT_DEG + HW - 1) / HW;
-    for (int q = nwin - 1; q >= 0; q--) {
-      const int b = q * HW;                    // HW = 16 divides 64
-      const uint32_t bits = (uint32_t) (p[b >> 6] >> (b & 63)) & 0xffffu;
-      if (t < MT_N) {
-        uint32_t v;
-        if (t < MT_N - HW) v = r0[t + HW];
-        else {
-          const int s = t - (MT_N - HW);
-          v = mt_f(r0[s], r0[s + 1], r0[MT_M + s]);
-        }
-#pragma unroll
-        for (int g = 0; g < HG; g++)
-          v ^= tab[(g * HTAB + ((bits >> (HSUB * g)) & (HTAB - 1))) * MT_N + t];
-        r1[t] = v;
-      }
-      __syncthreads();
-      uint32_t *tmp = r0; r0 = r1; r1 = tmp;
-    }
-    for (int k = t; k < MT_N; k += blockDim.x) ext[k] = r0[k];
     __syncthreads();
   }
-  uint32_t *dst = states_out + out_base * MT_N;
-  for (int k = t; k < MT_N; k += blockDim.x) dst[k] = ext[k];
 }
 
 // Block c generates draws [c*L, min((c+1)*L, count)) from window states[c].
@@ -462,7 +529,9 @@ int mt_prepare(int dev) {
     return EZMOCK_ERR_MEMORY;
   if (!EZ_CUDA_OK(cudaFuncSetAttribute(mt_horner_kernel,
           cudaFuncAttributeMaxDynamicSharedMemorySize,
-          (int) ((HG * HTAB * MT_N + 3 * MT_N + HW) * sizeof(uint32_t)))))
+          (int) H_SMEM)) ||
+      !EZ_CUDA_OK(cudaFuncSetAttribute(mt_jump_kernel,
+          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) HJ_SMEM)))
     return EZMOCK_ERR_UNKNOWN;
   g_mt_dev_ready = dev;
   return 0;
@@ -472,7 +541,8 @@ int mt_prepare(int dev) {
 // c < P = 2^p); its window is states[first + c].
 struct MtRange {
   uint64_t start, cap;
-  int l, p;
+  int l, p;                // chunk length 2^l; doubling plans: 2^p chunks
+  int P;                   // chunks
   size_t first;
 };
 
@@ -486,6 +556,7 @@ MtRange mt_plan(uint64_t start, uint64_t cap) {
   r.p = 0;
   while ((1ULL << r.l) * 128ULL < cap && r.l < 40) r.l++;
   while (((uint64_t) 1 << (r.l + r.p)) < cap) r.p++;
+  r.P = 1 << r.p;
   r.first = 0;
   return r;
 }
@@ -563,25 +634,166 @@ int mt_prepare_ranges(EzMesh *m, uint64_t seed, MtRange *r, int nr,
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
+// ---- direct jumps ----
+// Chunk c of a range starts at draw start + c L; its window is
+// (x^(start + c L) mod phi)(T) applied to the seed window.  The polynomials
+// depend only on (start, L), so the host computes them once (carry-less
+// products reduced modulo phi, ez_gf2.cpp) and keeps them on the device;
+// every fill then needs one Horner pass per chunk, all chunks in one launch,
+// instead of a jump followed by log2(chunks) dependent doubling levels.
+constexpr int MT_CHUNKS = 296;              // two waves of jump blocks
+
+bool g_gf2_tried = false, g_gf2_ok = false;
+
+// Under g_mt_mu with the tables built: set up the modular arithmetic and
+// check it against the squaring table (x^(2^(k+1)) = (x^(2^k))^2 mod phi).
+bool gf2_ready() {
+  if (g_gf2_tried) return g_gf2_ok;
+  g_gf2_tried = true;
+  if (!g_mt.ok || !ez_gf2_init(g_mt.phi.data(), MT_DEG, MT_PW)) return false;
+  std::vector<uint64_t> sq(MT_PW);
+  for (int k : {14, 15, 21, 40, 62}) {
+    ez_gf2_mulmod(&g_mt.xpow[(size_t) k * MT_PW], &g_mt.xpow[(size_t) k * MT_PW], sq.data());
+    if (memcmp(sq.data(), &g_mt.xpow[(size_t) (k + 1) * MT_PW], MT_PW * sizeof(uint64_t)))
+      return false;
+  }
+  g_gf2_ok = true;
+  return true;
+}
+
+struct JumpSeq {
+  std::vector<uint64_t> host;               // polynomials c = 0, 1, ...
+  uint64_t *dev = nullptr;                  // device copy of the first ndev
+  size_t ndev = 0;
+};
+std::map<std::tuple<int, uint64_t, int>, JumpSeq> g_jumps;   // (device, start, l)
+// replaced device copies: queued kernels may still read them, so they are
+// kept for the life of the process
+std::vector<uint64_t *> g_jumps_retired;
+
+// Under g_mt_mu, with device `dev` current: device polynomials
+// x^(start + c 2^l) mod phi for c < P.
+const uint64_t *jump_polys(int dev, uint64_t start, int l, size_t P) {
+  JumpSeq &js = g_jumps[std::make_tuple(dev, start, l)];
+  size_t nh = js.host.size() / MT_PW;
+  if (nh < P) {
+    js.host.resize(P * MT_PW);
+    uint64_t *h = js.host.data();
+    if (nh == 0) {
+      std::vector<uint64_t> t(MT_PW);
+      std::fill(h, h + MT_PW, 0);
+      h[0] = 1;                               // x^0
+      for (int k = 0; k < 64; k++)
+        if ((start >> k) & 1ULL) {
+          ez_gf2_mulmod(h, &g_mt.xpow[(size_t) k * MT_PW], t.data());
+          memcpy(h, t.data(), MT_PW * sizeof(uint64_t));
+        }
+      nh = 1;
+    }
+    for (size_t c = nh; c < P; c++)
+      ez_gf2_mulmod(h + (c - 1) * MT_PW, &g_mt.xpow[(size_t) l * MT_PW], h + c * MT_PW);
+  }
+  if (js.ndev < P) {
+    uint64_t *d = nullptr;
+    if (!EZ_CUDA_OK(cudaMalloc(&d, P * MT_PW * sizeof(uint64_t)))) { cudaGetLastError(); return nullptr; }
+    if (!EZ_CUDA_OK(cudaMemcpy(d, js.host.data(), P * MT_PW * sizeof(uint64_t),
+            cudaMemcpyHostToDevice))) {
+      cudaFree(d);
+      return nullptr;
+    }
+    if (js.dev) g_jumps_retired.push_back(js.dev);
+    js.dev = d;
+    js.ndev = P;
+  }
+  return js.dev;
+}
+
+// Chunk length 2^l >= 4096 so that at most `target` chunks cover `cap`.
+void plan_direct(MtRange &r, int target) {
+  if (target < 1) target = 1;
+  r.l = 12;
+  while (((r.cap + (1ULL << r.l) - 1) >> r.l) > (uint64_t) target && r.l < 62) r.l++;
+  r.P = (int) std::max<uint64_t>(1, (r.cap + (1ULL << r.l) - 1) >> r.l);
+  r.p = -1;
+  r.first = 0;
+}
+
+// Direct jumps available (tables built, modular arithmetic checked).
+bool mt_direct(int dev) {
+  if (mt_prepare(dev)) return false;
+  std::lock_guard<std::mutex> lk(g_mt_mu);
+  return gf2_ready();
+}
+
+// Chunk states of `nr` planned ranges: state `base` is the seed window, the
+// chunks of range i follow at r[i].first.  One launch, one block per chunk.
+int mt_prepare_direct(EzMesh *m, uint64_t seed, MtRange *r, int nr, size_t base) {
+  std::vector<MtJob> jobs;
+  size_t nst = 1;
+  {
+    std::lock_guard<std::mutex> lk(g_mt_mu);
+    for (int i = 0; i < nr; i++) {
+      r[i].first = base + nst;
+      const uint64_t *d = jump_polys(m->device, r[i].start, r[i].l, (size_t) r[i].P);
+      if (!d) return EZMOCK_ERR_MEMORY;
+      for (int c = 0; c < r[i].P; c++) {
+        MtJob j;
+        j.in = (uint32_t) base;
+        j.out = (uint32_t) (r[i].first + c);
+        j.poly = d + (size_t) c * MT_PW;
+        jobs.push_back(j);
+      }
+      nst += (size_t) r[i].P;
+    }
+  }
+  const size_t st_bytes = (base + nst) * MT_N * sizeof(uint32_t);
+  const size_t j_off = (st_bytes + 15) / 16 * 16;
+  int e = ez_rng_scratch(m, j_off + jobs.size() * sizeof(MtJob));
+  if (e) return e;
+  uint32_t *states = (uint32_t *) m->rng_scratch;
+  MtJob *d_jobs = (MtJob *) ((char *) m->rng_scratch + j_off);
+  std::vector<uint32_t> w(MT_N);
+  mt_seed_window(seed, w.data());
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(states + base * MT_N, w.data(), MT_N * sizeof(uint32_t),
+          cudaMemcpyHostToDevice, m->stream)) ||
+      !EZ_CUDA_OK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(MtJob),
+          cudaMemcpyHostToDevice, m->stream)))
+    return EZMOCK_ERR_UNKNOWN;
+  mt_jump_kernel<<<(unsigned) jobs.size(), H_THREADS, HJ_SMEM, m->stream>>>(states, d_jobs);
+  ez_count_launch();
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
 int mt_generate(EzMesh *m, const MtRange &r, uint64_t count, uint32_t *out) {
   if (!count) return 0;
   const uint32_t *states = (const uint32_t *) m->rng_scratch + r.first * MT_N;
   const uint64_t L = 1ULL << r.l;
-  const unsigned nb = (unsigned) ((count + L - 1) / L);
-  mt_gen_kernel<<<nb, G_THREADS, 0, m->stream>>>(states, L, count, out); ez_count_launch();
+  const uint64_t nb = (count + L - 1) / L;
+  if (nb > (uint64_t) r.P) return EZMOCK_ERR_UNKNOWN;
+  mt_ring_kernel<<<(unsigned) nb, R_THREADS, 0, m->stream>>>(states, L, count, out);
+  ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
 int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
     uint32_t *out, size_t base) {
   if (!count) return 0;
-  MtRange r = mt_plan(start, count);
-  int e = mt_prepare_ranges(m, seed, &r, 1, base);
+  MtRange r;
+  int e;
+  if (mt_direct(m->device)) {
+    r.start = start;
+    r.cap = count;
+    plan_direct(r, MT_CHUNKS);
+    e = mt_prepare_direct(m, seed, &r, 1, base);
+  }
+  else {
+    r = mt_plan(start, count);
+    e = mt_prepare_ranges(m, seed, &r, 1, base);
+  }
   if (e) return e;
   return mt_generate(m, r, count, out);
 }
 
-// Host copy of the seeding, used for the MT19937 raw-output check below.
 }  // namespace
 
 int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
@@ -601,15 +813,38 @@ int ez_rng_prepare(EzMesh *m, int ran, uint64_t seed, const uint64_t *starts,
   }
   if (ran == EZMOCK_RNG_MT19937) {
     MtRange r[EZ_RNG_MAXPREP];
-    for (int i = 0; i < n; i++) r[i] = mt_plan(starts[i], caps[i] ? caps[i] : 1);
-    const int e = mt_prepare_ranges(m, seed, r, n, 0);
+    int e;
+    if (mt_direct(m->device)) {
+      // one chunk length for all ranges (generation time is set by the
+      // longest chunk): the shortest whose chunks fit the block budget
+      int l = 12;
+      for (;; l++) {
+        uint64_t tot = 0;
+        for (int i = 0; i < n; i++)
+          tot += (std::max<uint64_t>(caps[i], 1) + (1ULL << l) - 1) >> l;
+        if (tot <= (uint64_t) MT_CHUNKS || l >= 62) break;
+      }
+      for (int i = 0; i < n; i++) {
+        r[i].start = starts[i];
+        r[i].cap = std::max<uint64_t>(caps[i], 1);
+        r[i].l = l;
+        r[i].P = (int) ((r[i].cap + (1ULL << l) - 1) >> l);
+        r[i].p = -1;
+        r[i].first = 0;
+      }
+      e = mt_prepare_direct(m, seed, r, n, 0);
+    }
+    else {
+      for (int i = 0; i < n; i++) r[i] = mt_plan(starts[i], caps[i] ? caps[i] : 1);
+      e = mt_prepare_ranges(m, seed, r, n, 0);
+    }
     if (e) return e;
     size_t end = 0;
     for (int i = 0; i < n; i++) {
       m->rng_prep[i].l = r[i].l;
-      m->rng_prep[i].p = r[i].p;
+      m->rng_prep[i].P = r[i].P;
       m->rng_prep[i].first = r[i].first;
-      end = std::max(end, r[i].first + ((size_t) 1 << r[i].p));
+      end = std::max(end, r[i].first + (size_t) r[i].P);
     }
     m->rng_prep_end = end;
   }
@@ -630,7 +865,8 @@ int ez_rng_fill_prepared(EzMesh *m, int ran, uint64_t seed, int i,
   r.start = m->rng_prep[i].start;
   r.cap = m->rng_prep[i].cap;
   r.l = m->rng_prep[i].l;
-  r.p = m->rng_prep[i].p;
+  r.P = m->rng_prep[i].P;
+  r.p = -1;
   r.first = m->rng_prep[i].first;
   return mt_generate(m, r, count, out);
 }
