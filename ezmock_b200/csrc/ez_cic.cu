@@ -127,39 +127,79 @@ __global__ void psi_absmax_kernel(const real *__restrict__ p, size_t n,
   if ((threadIdx.x & 31) == 0) atomicMax(&stats->psimax_bits, __float_as_uint(mx));
 }
 
+// Wraps an index that lies within one box length of [0, Ng).
+__device__ __forceinline__ int wrap1(int v, int Ng) {
+  return v < 0 ? v + Ng : (v >= Ng ? v - Ng : v);
+}
+
+// Float to integer on the FMA/ALU pipes instead of the conversion unit:
+// adding 1.5 * 2^23 places the integer part of |v| < 2^22 in the low
+// mantissa bits, rounded to nearest even (the default rounding of the add),
+// so the result equals __float2int_rn(v).
+constexpr float RMAGIC = 12582912.f;         // 1.5 * 2^23
+__device__ __forceinline__ int fround(float v) {
+  return __float_as_int(v + RMAGIC) - 0x4B400000;
+}
+// floor(v) for |v| < 2^22, exact: round, then step down where rounding went up.
+__device__ __forceinline__ int ffloor(float v) {
+  const float t = v + RMAGIC;
+  const float r = t - RMAGIC;                // v rounded to an integer, exact
+  return __float_as_int(t) - 0x4B400000 - (r > v ? 1 : 0);
+}
+
 __global__ void __launch_bounds__(OWN_NT, 2)
 cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
     const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
     int Ng, real igs, CicStats *stats, unsigned int *list) {
-  extern __shared__ int iring[];             // [4][OT*OT][ORS]
+  extern __shared__ __align__(16) int iring[];       // [4][OT*OT][ORS]
   const int nt = Ng / OT;
   const int i0 = (blockIdx.x / nt) * OT, j0 = (blockIdx.x % nt) * OT;
   // momentum scale: 1023 * max|psi| * scale < 2^31
   const float pmax = fmaxf(__uint_as_float(stats->psimax_bits), 1e-30f);
   const float mscale = exp2f(floorf(log2f(2147483647.f / (1024.f * pmax))));
   const float minv = 1.f / mscale;
-  for (int e = threadIdx.x; e < 4 * OQS; e += OWN_NT) iring[e] = 0;
+  for (int e = threadIdx.x; e < OQS; e += OWN_NT)
+    reinterpret_cast<int4 *>(iring)[e] = make_int4(0, 0, 0, 0);
   __syncthreads();
   const int nch = Ng / OKZ;
   const int lane = threadIdx.x & 31;
   for (int c = -1; c <= nch; c++) {
-    for (int p = threadIdx.x; p < OW * OW * OKZ; p += OWN_NT) {
+    // ring offsets of the chunks c-1, c, c+1 (slices 8(c-1) .. 8c+15)
+    const int rb0 = ((c + 2) % 3) * OKZ, rb1 = ((c + 3) % 3) * OKZ, rb2 = ((c + 4) % 3) * OKZ;
+    const bool cown = c >= 0 && c < nch;
+    // particle p's displacements are loaded one iteration ahead
+    auto locate = [&](int p, int &li, int &lj, int &zu, int &iw, int &jw, int &zw) {
       const int kz = p & (OKZ - 1), lc = p >> 3;
-      const int lj = lc % OW, li = lc / OW;
-      const int iu = i0 - OH + li, ju = j0 - OH + lj, zu = c * OKZ + kz;
-      const int iw = (iu + Ng) % Ng, jw = (ju + Ng) % Ng, zw = (zu + Ng) % Ng;
-      const size_t id = ((size_t) iw * Ng + jw) * Ng + zw;
-      const real pv[3] = {p0[id], p1[id], p2[id]};
-      // positions and weights exactly as dens_field.c:262-275
-      const real x = pv[0] * igs + iw, y = pv[1] * igs + jw, z = pv[2] * igs + zw;
-      const int x0 = (int) floor((double) x), y0 = (int) floor((double) y),
-                z0 = (int) floor((double) z);
-      const real wx1 = x - x0, wx0 = 1 - wx1;
-      const real wy1 = y - y0, wy0 = 1 - wy1;
-      const real wz1 = z - z0, wz0 = 1 - wz1;
+      li = lc / OW;
+      lj = lc - li * OW;
+      iw = wrap1(i0 - OH + li, Ng);
+      jw = wrap1(j0 - OH + lj, Ng);
+      zu = c * OKZ + kz;
+      zw = wrap1(zu, Ng);
+      return ((size_t) iw * Ng + jw) * Ng + zw;
+    };
+    int nli, nlj, nzu, niw, njw, nzw;
+    size_t nid = 0;
+    real na = 0, nb = 0, nc = 0;
+    if (threadIdx.x < OW * OW * OKZ) {
+      nid = locate(threadIdx.x, nli, nlj, nzu, niw, njw, nzw);
+      na = p0[nid]; nb = p1[nid]; nc = p2[nid];
+    }
+    for (int p = threadIdx.x; p < OW * OW * OKZ; p += OWN_NT) {
+      const int li = nli, lj = nlj, zu = nzu, iw = niw, jw = njw, zw = nzw;
+      const size_t id = nid;
+      const real pa = na, pb = nb, pc = nc;
+      if (p + OWN_NT < OW * OW * OKZ) {
+        nid = locate(p + OWN_NT, nli, nlj, nzu, niw, njw, nzw);
+        na = p0[nid]; nb = p1[nid]; nc = p2[nid];
+      }
+      // positions and weights as dens_field.c:262-275 (floor of a float is
+      // exact, so the single-precision floor equals the reference's)
+      const real x = pa * igs + iw, y = pb * igs + jw, z = pc * igs + zw;
+      const int x0 = ffloor(x), y0 = ffloor(y), z0 = ffloor(z);
       const int dx = x0 - iw, dy = y0 - jw, dz = z0 - zw;
       const bool far = dx < -OH || dx > OH || dy < -OH || dy > OH || dz < -OH || dz > OH;
-      const bool own = li >= OH && li < OH + OT && lj >= OH && lj < OH + OT && c >= 0 && c < nch;
+      const bool own = cown && li >= OH && li < OH + OT && lj >= OH && lj < OH + OT;
       const unsigned am = __activemask();
       const unsigned fm = __ballot_sync(am, far && own);
       if (fm) {
@@ -170,43 +210,68 @@ cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
         if (far && own) list[base + __popc(fm & ((1u << lane) - 1))] = (unsigned int) id;
       }
       if (far) continue;
-      const real wxs[2] = {wx0, wx1}, wys[2] = {wy0, wy1}, wzs[2] = {wz0, wz1};
+      // tile coordinates of the lower corner; skip particles whose cloud
+      // misses the tile
+      const int cx = li - OH + dx, cy = lj - OH + dy, zz = zu + dz;
+      const bool ax0 = (unsigned) cx < (unsigned) OT, ax1 = (unsigned) (cx + 1) < (unsigned) OT;
+      const bool by0 = (unsigned) cy < (unsigned) OT, by1 = (unsigned) (cy + 1) < (unsigned) OT;
+      const bool cz0 = (unsigned) zz < (unsigned) Ng, cz1 = (unsigned) (zz + 1) < (unsigned) Ng;
+      if (!((ax0 || ax1) && (by0 || by1) && (cz0 || cz1))) continue;
+      const real wx1 = x - x0, wx0 = 1 - wx1;
+      const real wy1 = y - y0, wy0 = 1 - wy1;
+      const real wz1 = z - z0, wz0 = 1 - wz1;
+      // slot of zz and zz + 1 in the ring (zz >> 3 is one of c-1, c, c+1)
+      const int k0 = (zz >> 3) - c, k1 = ((zz + 1) >> 3) - c;
+      const int s0 = (k0 < 0 ? rb0 : (k0 == 0 ? rb1 : rb2)) + (zz & (OKZ - 1));
+      const int s1 = (k1 < 0 ? rb0 : (k1 == 0 ? rb1 : rb2)) + ((zz + 1) & (OKZ - 1));
+      const int ox0 = cx * (OT * ORS), ox1 = ox0 + OT * ORS;
+      const int oy0 = cy * ORS, oy1 = oy0 + ORS;
+      // z weights scaled per quantity: rho, then the three momenta
+      const float sm1 = pa * mscale, sm2 = pb * mscale, sm3 = pc * mscale;
+      const float zr[2] = {wz0 * RHO_SCALE, wz1 * RHO_SCALE};
+      const float za[2] = {wz0 * sm1, wz1 * sm1};
+      const float zb[2] = {wz0 * sm2, wz1 * sm2};
+      const float zc[2] = {wz0 * sm3, wz1 * sm3};
+      const float wxy[4] = {wx0 * wy0, wx0 * wy1, wx1 * wy0, wx1 * wy1};
+      const bool okx[2] = {ax0, ax1}, oky[2] = {by0, by1}, okz[2] = {cz0, cz1};
+      const int oxs[2] = {ox0, ox1}, oys[2] = {oy0, oy1}, ss[2] = {s0, s1};
 #pragma unroll
-      for (int a = 0; a < 2; a++) {
-        const int cx = li - OH + dx + a;
-        if (cx < 0 || cx >= OT) continue;
+      for (int ab = 0; ab < 4; ab++) {
+        const int ia = ab >> 1, ib = ab & 1;
+        if (!(okx[ia] && oky[ib])) continue;
+        const int oxy = oxs[ia] + oys[ib];
+        const float w = wxy[ab];
 #pragma unroll
-        for (int b = 0; b < 2; b++) {
-          const int cy = lj - OH + dy + b;
-          if (cy < 0 || cy >= OT) continue;
-#pragma unroll
-          for (int cz = 0; cz < 2; cz++) {
-            const int zz = zu + dz + cz;
-            if (zz < 0 || zz >= Ng) continue;
-            const int slot = ((zz >> 3) % 3) * OKZ + (zz & (OKZ - 1));
-            const int base = (cx * OT + cy) * ORS + slot;
-            atomicAdd(iring + base, __float2int_rn(wxs[a] * wys[b] * wzs[cz] * RHO_SCALE));
-#pragma unroll
-            for (int d = 0; d < 3; d++)
-              atomicAdd(iring + (d + 1) * OQS + base,
-                  __float2int_rn((wxs[a] * pv[d]) * wys[b] * wzs[cz] * mscale));
-          }
+        for (int ic = 0; ic < 2; ic++) {
+          if (!okz[ic]) continue;
+          int *r = iring + oxy + ss[ic];
+          atomicAdd(r, fround(w * zr[ic]));
+          atomicAdd(r + OQS, fround(w * za[ic]));
+          atomicAdd(r + 2 * OQS, fround(w * zb[ic]));
+          atomicAdd(r + 3 * OQS, fround(w * zc[ic]));
         }
       }
     }
     __syncthreads();
     const int o = c - 1;                     // output chunk now complete
     if (o >= 0 && o < nch) {
-      for (int t = threadIdx.x; t < 4 * OT * OT * OKZ; t += OWN_NT) {
-        const int s = t & (OKZ - 1), col = (t >> 3) % (OT * OT), q = t / (OT * OT * OKZ);
-        const int idx = q * OQS + col * ORS + (o % 3) * OKZ + s;
-        const int v = iring[idx];
-        iring[idx] = 0;
-        if (q == 0 && v < 0) stats->overflow = 1;
+      // one (quantity, column) per thread and pass: 8 slices = two int4
+      const int ro = (o % 3) * OKZ;
+      for (int t = threadIdx.x; t < 4 * OT * OT; t += OWN_NT) {
+        const int q = t / (OT * OT), col = t - q * (OT * OT);
+        int4 *src = reinterpret_cast<int4 *>(iring + q * OQS + col * ORS + ro);
+        const int4 va = src[0], vb = src[1];
+        src[0] = make_int4(0, 0, 0, 0);
+        src[1] = make_int4(0, 0, 0, 0);
+        const float f = (q == 0) ? (1.f / RHO_SCALE) : minv;
+        if (q == 0 && (va.x | va.y | va.z | va.w | vb.x | vb.y | vb.z | vb.w) < 0)
+          stats->overflow = 1;
         real *g = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
         const int cx = col / OT, cy = col - cx * OT;
-        g[((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + o * OKZ + s] =
-            (q == 0) ? (real) v * (1.f / RHO_SCALE) : (real) v * minv;
+        float4 *dst = reinterpret_cast<float4 *>(
+            g + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + o * OKZ);
+        dst[0] = make_float4(va.x * f, va.y * f, va.z * f, va.w * f);
+        dst[1] = make_float4(vb.x * f, vb.y * f, vb.z * f, vb.w * f);
       }
     }
     __syncthreads();

@@ -148,6 +148,7 @@ void mesh_free_device(EzMesh *m) {
   if (m->scratch) cudaFree(m->scratch);
   if (m->rng_scratch) cudaFree(m->rng_scratch);
   if (m->fixacc) cudaFree(m->fixacc);
+  if (m->pkq) cudaFree(m->pkq);
   if (m->stats) cudaFree(m->stats);
   if (m->cat) cudaFree(m->cat);
   if (m->h_stage) cudaFreeHost(m->h_stage);

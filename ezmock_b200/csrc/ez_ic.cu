@@ -10,7 +10,8 @@
 // kernel needs no scattered writes.  The real parts at the seven non-origin
 // self-conjugate corners are zeroed (perturb.c:344-359).  All arithmetic is
 // FP64 (log, sqrt, sin, cos and the cubic-spline P(k)), rounded to `real` on
-// store, in the reference's expression order.
+// store, in the reference's expression order.  The interpolated P(k) is
+// tabulated per integer k^2 (pkq_kernel), which changes no result.
 #include "ez_internal.cuh"
 
 namespace {
@@ -46,23 +47,38 @@ __device__ __forceinline__ double pk_eval(const double *__restrict__ kt,
   return (lower + 0x1.5555555555555p-3 * (c + d)) / ba;
 }
 
+// The interpolated power depends on the cell only through the integer
+// ksq = ki^2 + kj^2 + k^2 (exact in double), so it is tabulated once per
+// field: q[ksq] = exp(P/2) for a log table, P otherwise (the per-cell
+// expressions below then apply exactly the reference's operations).
+__global__ void pkq_kernel(double *__restrict__ q, int nq,
+    const double *__restrict__ tab, int npk, int logpk, double kfac,
+    double logkfac) {
+  const double *kt = tab, *Pt = tab + npk, *P2 = tab + 2 * npk;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nq; s += gridDim.x * blockDim.x) {
+    if (s == 0) { q[0] = 0; continue; }       // the origin is never sampled
+    const double ksq = (double) s;
+    const double kmod = logpk ? log(ksq) * 0.5 + logkfac : kfac * sqrt(ksq);
+    const double P = pk_eval(kt, Pt, P2, npk, kmod);
+    q[s] = logpk ? exp(P * 0.5) : P;
+  }
+}
+
 __global__ void __launch_bounds__(IC_NT)
 ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
-    const double *__restrict__ tab, int npk, int logpk, int Ng, int Nk,
-    int Nkp, double kfac, double logkfac, double Pfac, int ran, int fixamp,
-    int iphase) {
+    const double *__restrict__ pkq, int logpk, int Ng, int Nk, int Nkp,
+    double kfac, double Pfac, int ran, int fixamp, int iphase) {
   const int Ngh = Ng >> 1;
   const int row = blockIdx.x;                       // i * Ng + j
   const int i = row / Ng, j = row - i * Ng;
-  const double ki = (i <= Ngh) ? i : i - Ng;
-  const double kj = (j <= Ngh) ? j : j - Ng;
+  const int ki = (i <= Ngh) ? i : i - Ng;
+  const int kj = (j <= Ngh) ? j : j - Ng;
   const int ni = (i == 0) ? 0 : Ng - i, nj = (j == 0) ? 0 : Ng - j;
-  const double kij = ki * ki + kj * kj;
+  const int kij = ki * ki + kj * kj;
   const bool lower = (i == ni && j <= Ngh) || (i != ni && i <= Ngh);
   const bool selfp = (i == ni && j == nj);
   const size_t rowc = (size_t) row * Nk;            // unpadded cell index base
   const size_t prowc = ((size_t) ni * Ng + nj) * Nk;
-  const double *kt = tab, *Pt = tab + npk, *P2 = tab + 2 * npk;
   const int per = fixamp ? 1 : 2;
   for (int k = threadIdx.x; k < Nkp; k += blockDim.x) {
     cplx out;
@@ -71,13 +87,15 @@ ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
     if (k < Nk && c != 0) {
       const bool plane = (k == 0) || (((Ng & 1) == 0) && k == Ngh);
       const size_t src = (!plane || lower) ? c : prowc + k;
-      const double ksq = kij + (double) (k * k);
-      const double kmod = logpk ? log(ksq) * 0.5 + logkfac : kfac * sqrt(ksq);
-      double P = pk_eval(kt, Pt, P2, npk, kmod);
-      double amp = 0;
-      if (!fixamp) amp = -log(ez_upos(ran, draws[(src - 1) * per]));
-      if (logpk) P = fixamp ? exp(P * 0.5) : exp(P * 0.5) * sqrt(amp);
-      else P = fixamp ? sqrt(P) : sqrt(P * amp);
+      const int isq = kij + k * k;
+      const double ksq = (double) isq;
+      const double Q = pkq[isq];
+      double P;
+      if (fixamp) P = logpk ? Q : sqrt(Q);
+      else {
+        const double amp = -log(ez_upos(ran, draws[(src - 1) * per]));
+        P = logpk ? Q * sqrt(amp) : sqrt(Q * amp);
+      }
       P *= Pfac;
       double phase = ez_u(ran, draws[(src - 1) * per + per - 1]) * 2 * EZ_PI;
       if (iphase) phase += EZ_PI;
@@ -99,25 +117,23 @@ ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
 // White-noise input: S = i sqrt(P)/(k^2 kf) L^-1.5 r2c(delta)
 // (perturb.c:476-554), applied to the forward transform already in S.
 __global__ void __launch_bounds__(IC_NT)
-wn_scale_kernel(cplx *__restrict__ S, const double *__restrict__ tab, int npk,
-    int logpk, int Ng, int Nk, int Nkp, double kfac, double logkfac,
-    double Pfac) {
+wn_scale_kernel(cplx *__restrict__ S, const double *__restrict__ pkq,
+    int logpk, int Ng, int Nk, int Nkp, double kfac, double Pfac) {
   const int Ngh = Ng >> 1;
   const int row = blockIdx.x;
   const int i = row / Ng, j = row - i * Ng;
-  const double ki = (i <= Ngh) ? i : i - Ng;
-  const double kj = (j <= Ngh) ? j : j - Ng;
-  const double kij = ki * ki + kj * kj;
-  const double *kt = tab, *Pt = tab + npk, *P2 = tab + 2 * npk;
+  const int ki = (i <= Ngh) ? i : i - Ng;
+  const int kj = (j <= Ngh) ? j : j - Ng;
+  const int kij = ki * ki + kj * kj;
   for (int k = threadIdx.x; k < Nkp; k += blockDim.x) {
     const size_t g = (size_t) row * Nkp + k;
     cplx w = S[g], out;
     out.x = 0; out.y = 0;
     if (k < Nk && !(row == 0 && k == 0)) {
-      const double ksq = kij + (double) (k * k);
-      const double kmod = logpk ? log(ksq) * 0.5 + logkfac : kfac * sqrt(ksq);
-      double P = pk_eval(kt, Pt, P2, npk, kmod);
-      P = logpk ? exp(P * 0.5) : sqrt(P);
+      const int isq = kij + k * k;
+      const double ksq = (double) isq;
+      double P = pkq[isq];
+      P = logpk ? P : sqrt(P);
       P *= Pfac / (ksq * kfac);
       out.x = -P * w.y;
       out.y = P * w.x;
@@ -128,6 +144,22 @@ wn_scale_kernel(cplx *__restrict__ S, const double *__restrict__ tab, int npk,
 
 }  // namespace
 
+namespace {
+// q[ksq] for ksq = 0 .. 3 (Ng/2)^2 on the mesh's device.
+int pkq_build(EzMesh *m, const EzPk *pk, double kfac, double logkfac) {
+  const int Ngh = m->Ng >> 1;
+  const int nq = 3 * Ngh * Ngh + 1;
+  if (!m->pkq && !EZ_CUDA_OK(cudaMalloc(&m->pkq, (size_t) nq * sizeof(double)))) {
+    m->pkq = nullptr;
+    cudaGetLastError();
+    return EZMOCK_ERR_MEMORY;
+  }
+  pkq_kernel<<<(nq + 255) / 256, 256, 0, m->stream>>>(m->pkq, nq, pk->d_tab, pk->n,
+      pk->log ? 1 : 0, kfac, logkfac); ez_count_launch();
+  return 0;
+}
+}  // namespace
+
 int ez_ic_spectrum(EzMesh *m, const EzPk *pk, double Lbox, int ran,
     int fixamp, int iphase, const uint32_t *draws) {
   const int Ng = m->Ng;
@@ -135,9 +167,11 @@ int ez_ic_spectrum(EzMesh *m, const EzPk *pk, double Lbox, int ran,
   const double logkfac = log(kfac);
   const double Pfac = pow(Lbox, -1.5);
   ez_stage_begin(m, ST_IC);
+  int e = pkq_build(m, pk, kfac, logkfac);
+  if (e) return e;
   ic_kernel<<<(unsigned) ((size_t) Ng * Ng), IC_NT, 0, m->stream>>>(
-      m->spec[0], draws, pk->d_tab, pk->n, pk->log ? 1 : 0, Ng, m->Nk, m->Nkp,
-      kfac, logkfac, Pfac, ran, fixamp, iphase); ez_count_launch();
+      m->spec[0], draws, m->pkq, pk->log ? 1 : 0, Ng, m->Nk, m->Nkp,
+      kfac, Pfac, ran, fixamp, iphase); ez_count_launch();
   ez_stage_end(m, ST_IC);
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
@@ -145,8 +179,10 @@ int ez_ic_spectrum(EzMesh *m, const EzPk *pk, double Lbox, int ran,
 int ez_wn_scale(EzMesh *m, const EzPk *pk, double Lbox) {
   const int Ng = m->Ng;
   const double kfac = EZ_PI * 2 / Lbox;
+  int e = pkq_build(m, pk, kfac, log(kfac));
+  if (e) return e;
   wn_scale_kernel<<<(unsigned) ((size_t) Ng * Ng), IC_NT, 0, m->stream>>>(
-      m->spec[0], pk->d_tab, pk->n, pk->log ? 1 : 0, Ng, m->Nk, m->Nkp, kfac,
-      log(kfac), pow(Lbox, -1.5)); ez_count_launch();
+      m->spec[0], m->pkq, pk->log ? 1 : 0, Ng, m->Nk, m->Nkp, kfac,
+      pow(Lbox, -1.5)); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }

@@ -102,6 +102,7 @@ struct EzMesh {
   int rng_nprep;           // prepared stream ranges (ez_rng_prepare)
   size_t rng_prep_end;     // first free state slot after them
   unsigned long long *fixacc;   // deterministic CIC accumulators (4 x N)
+  double *pkq;             // interpolated P(k) by integer k^2 (3 (Ng/2)^2 + 1)
   void *stats;             // EzCicStats on the device
   bool psimax_valid;       // stats->psimax_bits holds max |psi| of the fields
   real *cat;               // device catalogue (6 x cap)

@@ -105,33 +105,78 @@ scan_kernel(const unsigned long long *__restrict__ in, unsigned long long *out,
   if (threadIdx.x == 0) out[n] = tot;
 }
 
+// Box-Muller pairs of the bias stage (gauss_rand, pop_tracer.c:70-79): pair p
+// takes draws 2p (radius) and 2p+1 (angle) of the bias range; valid rank 2p
+// uses the cosine, 2p+1 the sine.  The multiplicative factor
+// G = 1 + g (g >= 0) or exp(g) (pop_tracer.c:288-300) is stored per rank.
 __global__ void __launch_bounds__(NT)
-bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
-    real thres, double iexp, double lambda, const unsigned long long *off,
-    const uint32_t *__restrict__ draws, int ran, unsigned long long *hist) {
-  __shared__ unsigned long long sw[32];
-  __shared__ unsigned int sh[EZ_NLOGB];
-  if (threadIdx.x < EZ_NLOGB) sh[threadIdx.x] = 0;
-  __syncthreads();
-  unsigned long long run = off[blockIdx.x];
-  const size_t b0 = (size_t) blockIdx.x * CH;
-  for (int q = 0; q < ROWS; q++) {
-    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    real r = 0;
-    bool valid = false;
-    if (id < N) { r = rho[id]; valid = !(r < thres); }
-    unsigned long long tot;
-    const unsigned long long rank = run + block_scan<unsigned long long>(valid ? 1ULL : 0ULL, &tot, sw);
-    run += tot;
-    if (id >= N) continue;
-    if (!valid) { rhot[id] = 0; continue; }
-    const real v = (r > (real) EZ_RHO_SAT) ? (real) EZ_RHO_SAT : r;
-    const unsigned long long p = rank >> 1;
+gauss_pair_kernel(const uint32_t *__restrict__ draws, size_t npair, int ran,
+    double lambda, double *__restrict__ G) {
+  for (size_t p = (size_t) blockIdx.x * NT + threadIdx.x; p < npair;
+       p += (size_t) gridDim.x * NT) {
     const double rr = -2 * log(ez_upos(ran, draws[2 * p]));
     const double th = ez_u(ran, draws[2 * p + 1]) * 2 * EZ_PI;
-    double g = (rank & 1) ? lambda * sqrt(rr) * sin(th) : lambda * sqrt(rr) * cos(th);
-    g = (g >= 0) ? 1 + g : exp(g);
-    const real t = (1 - exp((double) v * iexp)) * g;
+    const double s = lambda * sqrt(rr);
+    const double g0 = s * cos(th), g1 = s * sin(th);
+    G[2 * p] = (g0 >= 0) ? 1 + g0 : exp(g0);
+    G[2 * p + 1] = (g1 >= 0) ? 1 + g1 : exp(g1);
+  }
+}
+
+// rho_t of the valid cells of a 4096-cell chunk (pop_tracer.c:233-300).  A
+// cell's valid rank is the chunk offset plus the valid cells before it,
+// found from per-warp ballots.
+__global__ void __launch_bounds__(NT)
+bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
+    real thres, double iexp, const unsigned long long *off,
+    const double *__restrict__ G, unsigned long long *hist) {
+  constexpr int NW = NT / 32;
+  __shared__ unsigned int pre[ROWS * NW];    // valid counts, then prefixes
+  __shared__ unsigned int wsum[ROWS * NW / 32];
+  __shared__ unsigned int sh[EZ_NLOGB];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x < EZ_NLOGB) sh[threadIdx.x] = 0;
+  const size_t b0 = (size_t) blockIdx.x * CH;
+  real r[ROWS];
+  unsigned int bal[ROWS];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    r[q] = (id < N) ? rho[id] : (real) 0;
+    bal[q] = __ballot_sync(0xffffffffu, id < N && !(r[q] < thres));
+    if (lane == 0) pre[q * NW + w] = __popc(bal[q]);
+  }
+  __syncthreads();
+  // exclusive scan of the ROWS * NW counts (row-major: index order)
+  static_assert(ROWS * NW <= 32 * 32, "scan width");
+  unsigned int c = 0, incl = 0;
+  if (threadIdx.x < ROWS * NW) {
+    c = pre[threadIdx.x];
+    incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;
+  }
+  __syncthreads();
+  if (threadIdx.x < ROWS * NW) {
+    unsigned int base = 0;
+    for (int k = 0; k < w; k++) base += wsum[k];
+    pre[threadIdx.x] = base + incl - c;
+  }
+  __syncthreads();
+  const unsigned long long run = off[blockIdx.x];
+  const unsigned int lt = (1u << lane) - 1;
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    if (id >= N) continue;
+    if (!((bal[q] >> lane) & 1)) { rhot[id] = 0; continue; }
+    const unsigned long long rank = run + pre[q * NW + w] + __popc(bal[q] & lt);
+    const real v = (r[q] > (real) EZ_RHO_SAT) ? (real) EZ_RHO_SAT : r[q];
+    const real t = (1 - exp((double) v * iexp)) * G[rank];
     rhot[id] = t;
     atomicAdd(&sh[logb_bin(t)], 1u);
   }
@@ -688,8 +733,14 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   if ((e = ensure_draws(m, std::max(nd_bias, (size_t) 1)))) return e;
   if ((e = ez_rng_fill_prepared(m, ran, seed, 0, nd_bias, m->draws))) return e;
   cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
+  // G per valid rank in spec[1..2] (free until the selection's sort)
+  double *G = (double *) m->spec[1];
+  const size_t npair = nd_bias / 2;
+  if (npair)
+    gauss_pair_kernel<<<grid_for(npair, NT), NT, 0, st>>>(m->draws, npair, ran,
+        (double) (real) EZ_GAUSS_WIDTH, G); ez_count_launch();
   bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
-      (double) (real) EZ_GAUSS_WIDTH, bscan, m->draws, ran, hist); ez_count_launch();
+      bscan, G, hist); ez_count_launch();
   unsigned long long h[EZ_NLOGB];
   if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
