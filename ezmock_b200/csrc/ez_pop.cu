@@ -422,43 +422,97 @@ nt_kernel(const real *__restrict__ rhot, size_t N,
     nt[id] = (int16_t) cell_count(rhot[id], slo, sntr, nb);
 }
 
+// Tracer cells (pop_tracer.c:894-967): the tracers of a cell follow, in
+// cell-index order, those of all earlier cells.  The first index of each
+// cell comes from the chunk offset, per-(row, warp) prefixes and a warp scan
+// (skipped for the many warp rows without tracers); each tracer's cell index
+// is written to `cid`, and place_kernel computes the positions one thread per
+// tracer.
+template <typename cid_t>
 __global__ void __launch_bounds__(NT)
-emit_kernel(const real *__restrict__ rhot, size_t N, int Ng,
+tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
     const BoundOut *__restrict__ bo, const unsigned long long *__restrict__ off,
-    const uint32_t *__restrict__ draws, int ran, real gs, double Lbox,
-    unsigned long long ntr, real *x, real *y, real *z) {
+    unsigned long long ntr, cid_t *__restrict__ cid) {
+  constexpr int NW = NT / 32;
   __shared__ real slo[EZ_MAX_NT];
   __shared__ int sntr[EZ_MAX_NT];
-  __shared__ unsigned long long sw[32];
+  __shared__ unsigned int pre[ROWS * NW];
+  __shared__ unsigned int wsum[ROWS * NW / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nb = bo->nbins;
   for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
   __syncthreads();
-  unsigned long long run = off[blockIdx.x];
   const size_t b0 = (size_t) blockIdx.x * CH;
+  int n[ROWS];
+  unsigned int ex[ROWS];                       // exclusive prefix within the warp row
+#pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    const int n = (id < N) ? cell_count(rhot[id], slo, sntr, nb) : 0;
-    unsigned long long tot;
-    const unsigned long long t0 = run + block_scan<unsigned long long>((unsigned long long) n, &tot, sw);
-    run += tot;
-    if (!n) continue;
-    const int kk = (int) (id % Ng);
-    const size_t ij = id / Ng;
-    const int jj = (int) (ij % Ng), ii = (int) (ij / Ng);
-    for (int m = 0; m < n; m++) {
-      const unsigned long long t = t0 + m;
-      if (t >= ntr) break;
-      double r = ez_u(ran, draws[3 * t]) - 0.5;
-      real xx = (ii + r) * (double) gs;
-      r = ez_u(ran, draws[3 * t + 1]) - 0.5;
-      real yy = (jj + r) * (double) gs;
-      r = ez_u(ran, draws[3 * t + 2]) - 0.5;
-      real zz = (kk + r) * (double) gs;
-      if (xx < 0) xx = (double) xx + Lbox;
-      if (yy < 0) yy = (double) yy + Lbox;
-      if (zz < 0) zz = (double) zz + Lbox;
-      x[t] = xx; y[t] = yy; z[t] = zz;
+    n[q] = (id < N) ? cell_count(rhot[id], slo, sntr, nb) : 0;
+    unsigned int incl = (unsigned int) n[q];
+    if (__ballot_sync(0xffffffffu, n[q] != 0)) {
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
     }
+    ex[q] = incl - (unsigned int) n[q];
+    if (lane == 31) pre[q * NW + w] = incl;
+  }
+  __syncthreads();
+  unsigned int c = 0, incl = 0;
+  if (threadIdx.x < ROWS * NW) {
+    c = pre[threadIdx.x];
+    incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;
+  }
+  __syncthreads();
+  if (threadIdx.x < ROWS * NW) {
+    unsigned int base = 0;
+    for (int k = 0; k < w; k++) base += wsum[k];
+    pre[threadIdx.x] = base + incl - c;
+  }
+  __syncthreads();
+  const unsigned long long run = off[blockIdx.x];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    if (!n[q]) continue;
+    const cid_t id = (cid_t) (b0 + (size_t) q * NT + threadIdx.x);
+    const unsigned long long t0 = run + pre[q * NW + w] + ex[q];
+    for (int m = 0; m < n[q] && t0 + m < ntr; m++) cid[t0 + m] = id;
+  }
+}
+
+// Position of tracer t in its cell (pop_tracer.c:946-967): draws
+// 3t .. 3t+2 of the position range.
+template <typename cid_t>
+__global__ void __launch_bounds__(NT)
+place_kernel(const cid_t *__restrict__ cid, unsigned long long ntr, int Ng,
+    const uint32_t *__restrict__ draws, int ran, real gs, double Lbox,
+    real *x, real *y, real *z) {
+  for (unsigned long long t = (unsigned long long) blockIdx.x * NT + threadIdx.x; t < ntr;
+       t += (unsigned long long) gridDim.x * NT) {
+    const cid_t id = cid[t];
+    const cid_t ij = id / (cid_t) Ng;
+    const int kk = (int) (id - ij * (cid_t) Ng);
+    const cid_t ii = ij / (cid_t) Ng;
+    const int jj = (int) (ij - ii * (cid_t) Ng);
+    double r = ez_u(ran, draws[3 * t]) - 0.5;
+    real xx = ((int) ii + r) * (double) gs;
+    r = ez_u(ran, draws[3 * t + 1]) - 0.5;
+    real yy = (jj + r) * (double) gs;
+    r = ez_u(ran, draws[3 * t + 2]) - 0.5;
+    real zz = (kk + r) * (double) gs;
+    if (xx < 0) xx = (double) xx + Lbox;
+    if (yy < 0) yy = (double) yy + Lbox;
+    if (zz < 0) zz = (double) zz + Lbox;
+    x[t] = xx; y[t] = yy; z[t] = zz;
   }
 }
 
@@ -780,8 +834,23 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   if ((e = ensure_draws(m, std::max((size_t) 3 * nt_all, (size_t) 1)))) return e;
   if ((e = ez_rng_fill_prepared(m, ran, seed, 1, 3 * nt_all, m->draws))) return e;
   const real gs = Lbox / Ng;
-  emit_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, Ng, bo, bscan, m->draws,
-      ran, gs, Lbox, (unsigned long long) nt_all, cx, cy, cz); ez_count_launch();
+  // tracer cell indices in the velocity arrays (written later)
+  if (N <= 0xffffffffULL) {
+    uint32_t *cid = (uint32_t *) cvx;
+    tracer_cell_kernel<uint32_t><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
+        (unsigned long long) nt_all, cid); ez_count_launch();
+    if (nt_all)
+      place_kernel<uint32_t><<<grid_for(nt_all, NT), NT, 0, st>>>(cid, nt_all, Ng,
+          m->draws, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
+  }
+  else {
+    unsigned long long *cid = (unsigned long long *) cvx;      // vx and vy
+    tracer_cell_kernel<unsigned long long><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo,
+        bscan, (unsigned long long) nt_all, cid); ez_count_launch();
+    if (nt_all)
+      place_kernel<unsigned long long><<<grid_for(nt_all, NT), NT, 0, st>>>(cid, nt_all,
+          Ng, m->draws, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
+  }
   ez_stage_end(m, ST_EMIT);
 
   // ---- 5./6. velocities and dispersion ----
