@@ -321,14 +321,12 @@ fft_pass_k(const cplx *__restrict__ s0, const cplx *__restrict__ s1,
 // index XOR-swizzled by bits 4..7, which keeps both the strided line loads
 // and the bit-reversed stores (nearly) free of bank conflicts.
 
-__constant__ double2 c_w32[32];              // exp(+2 pi i k / 32)
+__constant__ cplx c_w32[32];                 // exp(+2 pi i k / 32), rounded to rt
 
 template <int S>
 __device__ __forceinline__ cplx w32(int k) {
-  const double2 w = c_w32[k & 31];
-  cplx r;
-  r.x = (rt) w.x;
-  r.y = (rt) (S * w.y);
+  cplx r = c_w32[k & 31];
+  if (S < 0) r.y = -r.y;
   return r;
 }
 
@@ -373,14 +371,45 @@ __device__ __forceinline__ void warp_fft(cplx *v, const cplx *tw, int lane) {
     if (S < 0) w.y = -w.y;
     v[k] = cmul(v[k], w);
   }
+  // Stage h: the lower lane keeps v + b, the upper lane (b - v) w with
+  // w = W_2h^(lane mod h).  Written as (s v + b) w_l with s = -1 and w_l = w
+  // on the upper lane, s = 1 and w_l = 1 on the lower one (exact).  The last
+  // two stages have w in {1, S i} and {1}: no complex multiply.
 #pragma unroll
-  for (int h = 16; h >= 1; h >>= 1) {
-    const cplx w = w32<S>((lane & (h - 1)) * (16 / h));
+  for (int h = 16; h >= 4; h >>= 1) {
     const bool hi = (lane & h) != 0;
+    const rt sg = hi ? (rt) -1 : (rt) 1;
+    cplx w = w32<S>((lane & (h - 1)) * (16 / h));
+    if (!hi) { w.x = 1; w.y = 0; }
 #pragma unroll
     for (int k = 0; k < E; k++) {
       const cplx b = shfl_xor_c(v[k], h);
-      v[k] = hi ? cmul(csub(b, v[k]), w) : cadd(v[k], b);
+      cplx t;
+      t.x = fma(sg, v[k].x, b.x);
+      t.y = fma(sg, v[k].y, b.y);
+      v[k] = cmul(t, w);
+    }
+  }
+  {
+    const rt sg = (lane & 2) ? (rt) -1 : (rt) 1;
+    const bool rot = (lane & 3) == 3;          // upper lane, w = W_4^1 = S i
+#pragma unroll
+    for (int k = 0; k < E; k++) {
+      const cplx b = shfl_xor_c(v[k], 2);
+      cplx t;
+      t.x = fma(sg, v[k].x, b.x);
+      t.y = fma(sg, v[k].y, b.y);
+      if (rot) { const rt x = t.x; t.x = -S * t.y; t.y = S * x; }
+      v[k] = t;
+    }
+  }
+  {
+    const rt sg = (lane & 1) ? (rt) -1 : (rt) 1;
+#pragma unroll
+    for (int k = 0; k < E; k++) {
+      const cplx b = shfl_xor_c(v[k], 1);
+      v[k].x = fma(sg, v[k].x, b.x);
+      v[k].y = fma(sg, v[k].y, b.y);
     }
   }
 }
@@ -717,11 +746,11 @@ bool w32_ready[64] = {false};
 bool set_w32(int dev) {
   if (dev < 0 || dev >= 64) return false;
   if (w32_ready[dev]) return true;
-  double2 h[32];
+  cplx h[32];
   const long double tpi = 6.283185307179586476925286766559005768L;
   for (int k = 0; k < 32; k++) {
-    h[k].x = (double) cosl(tpi * k / 32);
-    h[k].y = (double) sinl(tpi * k / 32);
+    h[k].x = (rt) cosl(tpi * k / 32);
+    h[k].y = (rt) sinl(tpi * k / 32);
   }
   if (!EZ_CUDA_OK(cudaMemcpyToSymbol(c_w32, h, sizeof(h)))) return false;
   w32_ready[dev] = true;
