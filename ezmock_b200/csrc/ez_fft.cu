@@ -24,6 +24,8 @@
 // Traffic: S read once; 2 + 3 spectra written, 5 read; 3 real fields written.
 #include "ez_internal.cuh"
 
+#include <cuda_pipeline.h>
+
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -433,11 +435,16 @@ wpass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
   const size_t pst = (size_t) Ng * Nkp;
-#pragma unroll 4
+  // the whole tile is copied asynchronously (no register staging), so all of
+  // a thread's loads are in flight at once
+#pragma unroll 8
   for (int e = threadIdx.x; e < n * WK; e += 32 * WNW) {
     const int i = e / WK, c = e - i * WK;
-    b0[c * LS + swz(i)] = S[i * pst + (size_t) j * Nkp + k0 + c];
+    __pipeline_memcpy_async(b0 + c * LS + swz(i), S + i * pst + (size_t) j * Nkp + k0 + c,
+        sizeof(cplx));
   }
+  __pipeline_commit();
+  __pipeline_wait_prior(0);
   __syncthreads();
   const int r = brev5(lane);
   for (int c = w; c < WK; c += WNW) {
@@ -486,13 +493,21 @@ wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
   const size_t base = (size_t) x * Ng * Nkp + k0;
-#pragma unroll 4
+  // asynchronous tile copies: A_x first (group 0), then A_0 (group 1), so B_x
+  // is transformed while A_0 is still arriving
+#pragma unroll 8
   for (int e = threadIdx.x; e < n * WK; e += 32 * WNW) {
     const int j = e / WK, c = e - j * WK;
-    const size_t g = base + (size_t) j * Nkp + c;
-    bx[c * LS + swz(j)] = s1[g];
-    b0[c * LS + swz(j)] = s2[g];
+    __pipeline_memcpy_async(bx + c * LS + swz(j), s1 + base + (size_t) j * Nkp + c, sizeof(cplx));
   }
+  __pipeline_commit();
+#pragma unroll 8
+  for (int e = threadIdx.x; e < n * WK; e += 32 * WNW) {
+    const int j = e / WK, c = e - j * WK;
+    __pipeline_memcpy_async(b0 + c * LS + swz(j), s2 + base + (size_t) j * Nkp + c, sizeof(cplx));
+  }
+  __pipeline_commit();
+  __pipeline_wait_prior(1);
   __syncthreads();
   const int r = brev5(lane);
   for (int c = w; c < WK; c += WNW) {
@@ -503,6 +518,11 @@ wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < E; k++) bx[c * LS + swz(k + E * r)] = v[k];
+  }
+  __pipeline_wait_prior(0);
+  __syncthreads();
+  for (int c = w; c < WK; c += WNW) {
+    cplx v[E];
 #pragma unroll
     for (int m = 0; m < E; m++) {
       const int jj = 32 * m + lane;

@@ -152,6 +152,7 @@ void mesh_free_device(EzMesh *m) {
   if (m->stats) cudaFree(m->stats);
   if (m->cat) cudaFree(m->cat);
   if (m->h_stage) cudaFreeHost(m->h_stage);
+  if (m->h_small) cudaFreeHost(m->h_small);
   for (int i = 0; i < 2; i++) if (m->d2h_ev[i]) cudaEventDestroy(m->d2h_ev[i]);
   if (m->stream) cudaStreamDestroy(m->stream);
   for (int i = 0; i < 2 * ST_NSTAGE; i++) if (m->ev[i]) cudaEventDestroy(m->ev[i]);

@@ -109,6 +109,7 @@ struct EzMesh {
   size_t cat_cap;
   size_t cat_n;            // length of the last catalogue (array stride)
   real *h_stage;           // pinned host staging for the catalogue
+  unsigned long long *h_small;  // pinned host staging for small uploads (EZ_MAX_NT words)
   size_t h_stage_cap;
   cudaEvent_t d2h_ev[2];   // staging halves ready
 };

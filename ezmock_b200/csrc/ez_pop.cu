@@ -711,9 +711,14 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
     }
     sorted = src;
   }
-  std::vector<unsigned long long> hp(nmax);
-  for (int j = 0; j < nmax; j++) hp[j] = pdf[j];
-  cudaMemcpyAsync(ps.dpdf, hp.data(), nmax * 8, cudaMemcpyHostToDevice, st);
+  // the PDF goes through pinned memory: a pageable upload would wait for
+  // the stream (the buffer is reused only after this stage's final wait)
+  if (!m->h_small && !EZ_CUDA_OK(cudaMallocHost(&m->h_small, EZ_MAX_NT * sizeof(unsigned long long)))) {
+    m->h_small = nullptr;
+    return EZMOCK_ERR_MEMORY;
+  }
+  for (int j = 0; j < nmax; j++) m->h_small[j] = pdf[j];
+  cudaMemcpyAsync(ps.dpdf, m->h_small, nmax * 8, cudaMemcpyHostToDevice, st);
   bounds_kernel<<<1, 1, 0, st>>>(sorted, M, ps.dpdf, nmax, ncell, ntot, ps.bo); ez_count_launch();
   if (!EZ_CUDA_OK(cudaMemcpyAsync(hb, ps.bo, sizeof(*hb), cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
@@ -764,6 +769,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   cudaStream_t st = m->stream;
 
   // random streams of the three stages, prepared together (MT19937 jumps)
+  ez_stage_begin(m, ST_BIAS);
   {
     const uint64_t nt_cap = ntot + ntot / 32 + 1024;
     const uint64_t starts[3] = {(uint64_t) N << 1, (uint64_t) N * 5, (uint64_t) N << 3};
@@ -772,7 +778,6 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   }
 
   // ---- 1. valid ranks ----
-  ez_stage_begin(m, ST_BIAS);
   valid_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, N, thres, bcnt); ez_count_launch();
   scan_u64(bcnt, bscan, nblk, ps.tmp, st);
   unsigned long long nvalid = 0;

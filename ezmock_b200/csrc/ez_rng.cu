@@ -310,28 +310,36 @@ mt_horner_kernel(uint32_t *states, const int4 *__restrict__ desc,
   for (int k = t; k < MT_N; k += blockDim.x) dst[k] = ext[k];
 }
 
-// One direct jump per block: states[job.out] = job.poly(T) states[job.in].
-struct MtJob {
-  uint32_t in, out;
-  const uint64_t *poly;                      // MT_PW words, x^J mod phi
+// Direct jumps of up to four ranges from one seed window, passed by value
+// (no host-to-device copy, hence no stream synchronisation): block b of range
+// i computes chunk c = b - (blocks of earlier ranges) and writes
+// states[first[i] + c] = (poly[i] + c MT_PW)(T) seed.
+constexpr int MT_MAXR = 4;
+struct MtJumpArgs {
+  uint32_t w[MT_N];                          // seed window
+  int nr;
+  int P[MT_MAXR];                            // chunks per range
+  uint32_t first[MT_MAXR];                   // state index of chunk 0
+  const uint64_t *poly[MT_MAXR];             // P polynomials each
 };
 
 __global__ void __launch_bounds__(H_THREADS)
-mt_jump_kernel(uint32_t *states, const MtJob *__restrict__ jobs) {
+mt_jump_kernel(uint32_t *states, const MtJumpArgs a) {
   extern __shared__ uint32_t sm[];
-  const MtJob job = jobs[blockIdx.x];
+  int i = 0, c = blockIdx.x;
+  while (i < a.nr - 1 && c >= a.P[i]) { c -= a.P[i]; i++; }
+  const uint64_t *poly = a.poly[i] + (size_t) c * MT_PW;
   uint32_t *tab = sm;
   uint32_t *ext = tab + HG * HTAB * MT_N;
   uint32_t *ra = ext + MT_N + HW;
   uint32_t *rb = ra + MT_N;
   uint64_t *pp = (uint64_t *) (sm + H_SMEM_WORDS + (H_SMEM_WORDS & 1));
   const int t = threadIdx.x;
-  const uint32_t *src = states + (size_t) job.in * MT_N;
-  for (int k = t; k < MT_N; k += blockDim.x) ext[k] = src[k];
-  for (int k = t; k < MT_PW; k += blockDim.x) pp[k] = job.poly[k];
+  for (int k = t; k < MT_N; k += blockDim.x) ext[k] = a.w[k];
+  for (int k = t; k < MT_PW; k += blockDim.x) pp[k] = poly[k];
   __syncthreads();
   horner_apply(ext, tab, ra, rb, pp);
-  uint32_t *dst = states + (size_t) job.out * MT_N;
+  uint32_t *dst = states + (size_t) (a.first[i] + c) * MT_N;
   for (int k = t; k < MT_N; k += blockDim.x) dst[k] = ext[k];
 }
 
@@ -725,42 +733,31 @@ bool mt_direct(int dev) {
   return gf2_ready();
 }
 
-// Chunk states of `nr` planned ranges: state `base` is the seed window, the
-// chunks of range i follow at r[i].first.  One launch, one block per chunk.
+// Chunk states of `nr` <= MT_MAXR planned ranges; the chunks of range i are
+// stored from state index r[i].first = base + (chunks of earlier ranges).
+// One launch, one block per chunk.
 int mt_prepare_direct(EzMesh *m, uint64_t seed, MtRange *r, int nr, size_t base) {
-  std::vector<MtJob> jobs;
-  size_t nst = 1;
+  if (nr > MT_MAXR) return EZMOCK_ERR_UNKNOWN;
+  MtJumpArgs a;
+  a.nr = nr;
+  size_t nst = 0;
   {
     std::lock_guard<std::mutex> lk(g_mt_mu);
     for (int i = 0; i < nr; i++) {
       r[i].first = base + nst;
       const uint64_t *d = jump_polys(m->device, r[i].start, r[i].l, (size_t) r[i].P);
       if (!d) return EZMOCK_ERR_MEMORY;
-      for (int c = 0; c < r[i].P; c++) {
-        MtJob j;
-        j.in = (uint32_t) base;
-        j.out = (uint32_t) (r[i].first + c);
-        j.poly = d + (size_t) c * MT_PW;
-        jobs.push_back(j);
-      }
+      a.P[i] = r[i].P;
+      a.first[i] = (uint32_t) r[i].first;
+      a.poly[i] = d;
       nst += (size_t) r[i].P;
     }
   }
-  const size_t st_bytes = (base + nst) * MT_N * sizeof(uint32_t);
-  const size_t j_off = (st_bytes + 15) / 16 * 16;
-  int e = ez_rng_scratch(m, j_off + jobs.size() * sizeof(MtJob));
+  int e = ez_rng_scratch(m, (base + nst) * MT_N * sizeof(uint32_t));
   if (e) return e;
-  uint32_t *states = (uint32_t *) m->rng_scratch;
-  MtJob *d_jobs = (MtJob *) ((char *) m->rng_scratch + j_off);
-  std::vector<uint32_t> w(MT_N);
-  mt_seed_window(seed, w.data());
-  if (!EZ_CUDA_OK(cudaMemcpyAsync(states + base * MT_N, w.data(), MT_N * sizeof(uint32_t),
-          cudaMemcpyHostToDevice, m->stream)) ||
-      !EZ_CUDA_OK(cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(MtJob),
-          cudaMemcpyHostToDevice, m->stream)))
-    return EZMOCK_ERR_UNKNOWN;
-  mt_jump_kernel<<<(unsigned) jobs.size(), H_THREADS, HJ_SMEM, m->stream>>>(states, d_jobs);
-  ez_count_launch();
+  mt_seed_window(seed, a.w);
+  mt_jump_kernel<<<(unsigned) nst, H_THREADS, HJ_SMEM, m->stream>>>(
+      (uint32_t *) m->rng_scratch, a); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
