@@ -103,7 +103,8 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []                 # (host time, csv line)
+        self.window = None
 
     def start(self):
         try:
@@ -118,7 +119,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark(self, t0, t1):
+        """Keep only samples taken between host times t0 and t1 (the timed
+        region); the sampler itself starts before the warm-up so that its
+        start-up does not fall inside the timed region."""
+        self.window = (t0, t1)
 
     def stop(self):
         if not self.proc:
@@ -131,7 +138,12 @@ class ClockSampler:
         self.th.join(timeout=2)
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = [ln for t, ln in self.lines
+                 if self.window is None or self.window[0] <= t <= self.window[1]]
+        if not lines and self.lines:     # timed region shorter than one period
+            t_mid = 0.5 * (self.window[0] + self.window[1])
+            lines = [min(self.lines, key=lambda x: abs(x[0] - t_mid))[1]]
+        for ln in lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -266,12 +278,12 @@ def main():
         n = m.populate_device(*params, nexp)
         return n, stage_c
 
+    clk = ClockSampler(local)
+    clk.start()
     for _ in range(args.warmup):
         device_step()
     m.sync()
     barrier()
-    clk = ClockSampler(local)
-    clk.start()
     l0 = L.EZmockB200_launch_count()
     L.EZmockB200_mark(m._ez, 0)
     t0 = time.perf_counter()
@@ -289,6 +301,7 @@ def main():
     L.EZmockB200_elapsed(m._ez, 0, 1, ctypes.byref(ms))
     wall = time.perf_counter() - t0
     launches = L.EZmockB200_launch_count() - l0
+    clk.mark(t0, t0 + wall)
     clocks = clk.stop()
     barrier()
     t_dev = reduce_max(ms.value / 1e3)

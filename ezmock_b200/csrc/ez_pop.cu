@@ -169,14 +169,21 @@ bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
   __syncthreads();
   const unsigned long long run = off[blockIdx.x];
   const unsigned int lt = (1u << lane) - 1;
+  // all G loads first (rank order follows index order, so they coalesce)
+  double g[ROWS];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const bool valid = (bal[q] >> lane) & 1;
+    const unsigned long long rank = run + pre[q * NW + w] + __popc(bal[q] & lt);
+    g[q] = valid ? G[rank] : 0.0;
+  }
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     if (id >= N) continue;
     if (!((bal[q] >> lane) & 1)) { rhot[id] = 0; continue; }
-    const unsigned long long rank = run + pre[q * NW + w] + __popc(bal[q] & lt);
     const real v = (r[q] > (real) EZ_RHO_SAT) ? (real) EZ_RHO_SAT : r[q];
-    const real t = (1 - exp((double) v * iexp)) * G[rank];
+    const real t = (1 - exp((double) v * iexp)) * g[q];
     rhot[id] = t;
     atomicAdd(&sh[logb_bin(t)], 1u);
   }
@@ -400,9 +407,16 @@ tracer_count_kernel(const real *__restrict__ rhot, size_t N,
   __syncthreads();
   unsigned long long c = 0;
   const size_t b0 = (size_t) blockIdx.x * CH;
+  real v[ROWS];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {               // all loads first
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    v[q] = (id < N) ? rhot[id] : (real) 0;
+  }
+#pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    if (id < N) c += cell_count(rhot[id], slo, sntr, nb);
+    if (id < N) c += cell_count(v[q], slo, sntr, nb);
   }
   unsigned long long tot;
   block_scan<unsigned long long>(c, &tot, sw);
@@ -445,10 +459,16 @@ tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
   const size_t b0 = (size_t) blockIdx.x * CH;
   int n[ROWS];
   unsigned int ex[ROWS];                       // exclusive prefix within the warp row
+  real v[ROWS];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {               // all loads first
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    v[q] = (id < N) ? rhot[id] : (real) 0;
+  }
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    n[q] = (id < N) ? cell_count(rhot[id], slo, sntr, nb) : 0;
+    n[q] = (id < N) ? cell_count(v[q], slo, sntr, nb) : 0;
     unsigned int incl = (unsigned int) n[q];
     if (__ballot_sync(0xffffffffu, n[q] != 0)) {
 #pragma unroll
