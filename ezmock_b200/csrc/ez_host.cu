@@ -140,6 +140,7 @@ void pk_free(EzPk *p) {
 }
 
 void mesh_free_device(EzMesh *m) {
+  if (m->side) cudaStreamSynchronize(m->side);
   if (m->spec[0]) cudaFree(m->spec[0]);
   if (m->psi[0]) cudaFree(m->psi[0]);
   if (m->rho) cudaFree(m->rho);
@@ -155,9 +156,28 @@ void mesh_free_device(EzMesh *m) {
   if (m->h_small) cudaFreeHost(m->h_small);
   for (int i = 0; i < 2; i++) if (m->d2h_ev[i]) cudaEventDestroy(m->d2h_ev[i]);
   if (m->stream) cudaStreamDestroy(m->stream);
+  if (m->side) cudaStreamDestroy(m->side);
+  if (m->ev_main) cudaEventDestroy(m->ev_main);
+  if (m->ev_side) cudaEventDestroy(m->ev_side);
+  if (m->rng_side) cudaFree(m->rng_side);
+  if (m->draws_bias) cudaFree(m->draws_bias);
   for (int i = 0; i < 2 * ST_NSTAGE; i++) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
   for (int i = 0; i < 8; i++) if (m->mark[i]) cudaEventDestroy(m->mark[i]);
 }
+
+// The population stages' random streams for the instance seed (bias draws
+// 2N.., positions 5N.., dispersion 8N..; pop_tracer.c:233-237, :919, :1071),
+// prepared on the side stream while the field is created.  The position and
+// dispersion capacities are those of the last population of the instance.
+void side_streams(EZMOCK *ez) {
+  EzMesh *m = MESH(ez);
+  const uint64_t N = m->N, h = m->pop_hint;
+  const uint64_t starts[3] = {N << 1, N * 5, N << 3};
+  const uint64_t caps[3] = {N + 2, 3 * h, 6 * ((h + 1) / 2)};
+  ez_rng_side_prepare(m, RNG(ez)->ran, RNG(ez)->seed, starts, caps, h ? 3 : 1, N + 2);
+}
+
+void side_streams_cb(void *ez) { side_streams((EZMOCK *) ez); }
 
 int set_device(EzMesh *m) {
   return EZ_CUDA_OK(cudaSetDevice(m->device)) ? 0 : EZMOCK_ERR_UNKNOWN;
@@ -296,8 +316,13 @@ void ez_stage_end(EzMesh *m, int st) {
 int ez_mesh_alloc(EzMesh *m, int Ng) {
   if (m->spec[0]) return 0;
   if (!EZ_CUDA_OK(cudaSetDevice(m->device))) return EZMOCK_ERR_UNKNOWN;
-  if (!m->stream && !EZ_CUDA_OK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking)))
-    return EZMOCK_ERR_UNKNOWN;
+  if (!m->stream) {
+    // highest priority: the side stream's preparations yield to it
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (!EZ_CUDA_OK(cudaStreamCreateWithPriority(&m->stream, cudaStreamNonBlocking, hi)))
+      return EZMOCK_ERR_UNKNOWN;
+  }
   for (int i = 0; i < 2 * ST_NSTAGE; i++)
     if (!m->ev[i] && !EZ_CUDA_OK(cudaEventCreate(&m->ev[i]))) return EZMOCK_ERR_UNKNOWN;
   m->Ng = Ng;
@@ -542,7 +567,8 @@ int EZmock_create_dens_field(EZMOCK *ez, real *psi[3], bool deepcopy,
     else {
       const size_t ndraw = ((size_t) conf->Ng * conf->Ng * m->Nk - 1) * (fixamp ? 1 : 2);
       ez_stage_begin(m, ST_RNG_IC);
-      if ((e = ez_rng_fill(m, RNG(ez)->ran, RNG(ez)->seed, 0, ndraw, m->draws)))
+      if ((e = ez_rng_fill_around(m, RNG(ez)->ran, RNG(ez)->seed, 0, ndraw, m->draws,
+              side_streams_cb, ez)))
         return (*err = e);
       ez_stage_end(m, ST_RNG_IC);
       if ((e = ez_ic_spectrum(m, pk, conf->Lbox, RNG(ez)->ran, fixamp, iphase, m->draws)) ||
@@ -551,6 +577,7 @@ int EZmock_create_dens_field(EZMOCK *ez, real *psi[3], bool deepcopy,
     }
     m->psi_ref = false;
   }
+  if (user_psi || delta) side_streams(ez);
   if ((e = ez_cic(m, conf->Lbox))) return (*err = e);
   if (!EZ_CUDA_OK(cudaStreamSynchronize(m->stream))) return (*err = EZMOCK_ERR_UNKNOWN);
   m->fixamp = fixamp;

@@ -98,9 +98,23 @@ struct EzMesh {
   size_t scratch_cap;
   void *rng_scratch;       // skip-ahead states of the MT19937 streams
   size_t rng_scratch_cap;
-  struct { uint64_t start, cap; int l, P; size_t first; } rng_prep[4];  // P chunks of 2^l
+  struct EzRange { uint64_t start, cap; int l, P; size_t first; bool side; };
+  EzRange rng_prep[4];     // P chunks of 2^l; states in rng_side when `side`
   int rng_nprep;           // prepared stream ranges (ez_rng_prepare)
   size_t rng_prep_end;     // first free state slot after them
+  // side stream: the population stages' random streams for the current seed,
+  // prepared while the field is being created (ez_rng_side_prepare)
+  cudaStream_t side;
+  cudaEvent_t ev_main, ev_side;
+  uint32_t *rng_side;      // chunk states of the side ranges
+  size_t rng_side_cap;     // bytes
+  uint32_t *draws_bias;    // draws of side range 0 (the bias stage)
+  size_t draws_bias_cap;   // uint32 values
+  bool pre_valid;
+  int pre_ran, pre_n;
+  uint64_t pre_seed, pre_bias_n;
+  EzRange pre[3];
+  size_t pop_hint;         // tracer capacity of the last population (0: none)
   unsigned long long *fixacc;   // deterministic CIC accumulators (4 x N)
   double *pkq;             // interpolated P(k) by integer k^2 (3 (Ng/2)^2 + 1)
   void *stats;             // EzCicStats on the device
@@ -129,14 +143,27 @@ struct EzCicStats {
 // Raw 32-bit draws [start, start+count) of the stream seeded by `seed`.
 int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
     uint64_t count, uint32_t *out);
+// ez_rng_fill that calls between(arg) once the work generating the draws no
+// longer needs the whole GPU (MT19937: after the chunk jumps, before the
+// generation), so that work launched there can share the SMs with it.
+int ez_rng_fill_around(EzMesh *m, int ran, uint64_t seed, uint64_t start,
+    uint64_t count, uint32_t *out, void (*between)(void *), void *arg);
 // Prepares the ranges [starts[i], starts[i] + caps[i]) of one stream so that
 // later fills of them skip the jump (MT19937 chunk states computed together).
 #define EZ_RNG_MAXPREP 4
 int ez_rng_prepare(EzMesh *m, int ran, uint64_t seed, const uint64_t *starts,
     const uint64_t *caps, int n);
-// Draws [starts[i], starts[i] + count) of prepared range i.
-int ez_rng_fill_prepared(EzMesh *m, int ran, uint64_t seed, int i,
-    uint64_t count, uint32_t *out);
+// Draws [starts[i], starts[i] + count) of prepared range i: *res points to
+// them, either in `out` (generated on the instance stream) or in the side
+// stream's buffer.
+int ez_rng_draws(EzMesh *m, int ran, uint64_t seed, int i, uint64_t count,
+    uint32_t *out, const uint32_t **res);
+// On the instance's low-priority side stream, after the instance stream's
+// work so far: chunk states of the ranges [starts[i], starts[i] + caps[i])
+// (MT19937) and the first `nbias` draws of range 0.  Failures only leave
+// the side results unused.
+void ez_rng_side_prepare(EzMesh *m, int ran, uint64_t seed,
+    const uint64_t *starts, const uint64_t *caps, int n, uint64_t nbias);
 // Conversions shared by all kernels (prand definitions of the oracle):
 //   MT19937  : u = x 2^-32 in [0,1); u_pos = (x + 0.5) 2^-32 in (0,1)
 //   MRG32k3a : u = u_pos = x * 2.328306549295727688e-10 in (0,1)

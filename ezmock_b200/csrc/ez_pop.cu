@@ -792,6 +792,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   ez_stage_begin(m, ST_BIAS);
   {
     const uint64_t nt_cap = ntot + ntot / 32 + 1024;
+    m->pop_hint = nt_cap;                 // capacity for the next field's side streams
     const uint64_t starts[3] = {(uint64_t) N << 1, (uint64_t) N * 5, (uint64_t) N << 3};
     const uint64_t caps[3] = {(uint64_t) N + 2, 3 * nt_cap, 6 * ((nt_cap + 1) / 2)};
     if ((e = ez_rng_prepare(m, ran, seed, starts, caps, 3))) return e;
@@ -810,13 +811,14 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // ---- 2. bias ----
   const size_t nd_bias = nvalid + (nvalid & 1);
   if ((e = ensure_draws(m, std::max(nd_bias, (size_t) 1)))) return e;
-  if ((e = ez_rng_fill_prepared(m, ran, seed, 0, nd_bias, m->draws))) return e;
+  const uint32_t *dbias = nullptr;
+  if ((e = ez_rng_draws(m, ran, seed, 0, nd_bias, m->draws, &dbias))) return e;
   cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
   // G per valid rank in spec[1..2] (free until the selection's sort)
   double *G = (double *) m->spec[1];
   const size_t npair = nd_bias / 2;
   if (npair)
-    gauss_pair_kernel<<<grid_for(npair, NT), NT, 0, st>>>(m->draws, npair, ran,
+    gauss_pair_kernel<<<grid_for(npair, NT), NT, 0, st>>>(dbias, npair, ran,
         (double) (real) EZ_GAUSS_WIDTH, G); ez_count_launch();
   bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
       bscan, G, hist); ez_count_launch();
@@ -857,7 +859,8 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // the per-cell counts must add up to the selected total (pop_tracer.c:989-993)
   if (ncount != nt_all) { res->err = EZMOCK_ERR_UNKNOWN; return 0; }
   if ((e = ensure_draws(m, std::max((size_t) 3 * nt_all, (size_t) 1)))) return e;
-  if ((e = ez_rng_fill_prepared(m, ran, seed, 1, 3 * nt_all, m->draws))) return e;
+  const uint32_t *dpos = nullptr;
+  if ((e = ez_rng_draws(m, ran, seed, 1, 3 * nt_all, m->draws, &dpos))) return e;
   const real gs = Lbox / Ng;
   // tracer cell indices in the velocity arrays (written later)
   if (N <= 0xffffffffULL) {
@@ -866,7 +869,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
         (unsigned long long) nt_all, cid); ez_count_launch();
     if (nt_all)
       place_kernel<uint32_t><<<grid_for(nt_all, NT), NT, 0, st>>>(cid, nt_all, Ng,
-          m->draws, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
+          dpos, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
   }
   else {
     unsigned long long *cid = (unsigned long long *) cvx;      // vx and vy
@@ -874,7 +877,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
         bscan, (unsigned long long) nt_all, cid); ez_count_launch();
     if (nt_all)
       place_kernel<unsigned long long><<<grid_for(nt_all, NT), NT, 0, st>>>(cid, nt_all,
-          Ng, m->draws, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
+          Ng, dpos, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
   }
   ez_stage_end(m, ST_EMIT);
 
@@ -885,8 +888,9 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
       m->paint[1], m->paint[2], Ng, igs, vfac, nt_all, cx, cy, cz, cvx, cvy, cvz); ez_count_launch();
   const size_t nd_disp = 6 * ((nt_all + 1) / 2);
   if ((e = ensure_draws(m, std::max(nd_disp, (size_t) 1)))) return e;
-  if ((e = ez_rng_fill_prepared(m, ran, seed, 2, nd_disp, m->draws))) return e;
-  disp_kernel<<<grid_for((nt_all + 1) / 2, NT), NT, 0, st>>>(nt_all, m->draws,
+  const uint32_t *ddisp = nullptr;
+  if ((e = ez_rng_draws(m, ran, seed, 2, nd_disp, m->draws, &ddisp))) return e;
+  disp_kernel<<<grid_for((nt_all + 1) / 2, NT), NT, 0, st>>>(nt_all, ddisp,
       ran, (double) sigma_v, cvx, cvy, cvz); ez_count_launch();
   ez_stage_end(m, ST_VEL);
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;

@@ -190,9 +190,9 @@ int mrg_prepare(int dev) {
   return 0;
 }
 
-int mrg_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
-    uint32_t *out) {
-  int e = mrg_prepare(m->device);
+int mrg_fill_st(int dev, cudaStream_t st, uint64_t seed, uint64_t start,
+    uint64_t count, uint32_t *out) {
+  int e = mrg_prepare(dev);
   if (e) return e;
   uint64_t z = seed, s1[3], s2[3];
   for (int j = 0; j < 3; j++) s1[j] = splitmix64(&z) % M1;
@@ -201,10 +201,15 @@ int mrg_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
   if (!s2[0] && !s2[1] && !s2[2]) s2[0] = 1;
   const uint64_t nblk = (count + MRG_BLOCK - 1) / MRG_BLOCK;
   if (!nblk) return 0;
-  mrg_fill_kernel<<<(unsigned) nblk, MRG_THREADS, 0, m->stream>>>(
+  mrg_fill_kernel<<<(unsigned) nblk, MRG_THREADS, 0, st>>>(
       (uint32_t) s1[0], (uint32_t) s1[1], (uint32_t) s1[2], (uint32_t) s2[0],
       (uint32_t) s2[1], (uint32_t) s2[2], start, count, g_mrg_thread_jump, out); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+int mrg_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
+    uint32_t *out) {
+  return mrg_fill_st(m->device, m->stream, seed, start, count, out);
 }
 
 // ============================================================================
@@ -734,9 +739,11 @@ bool mt_direct(int dev) {
 }
 
 // Chunk states of `nr` <= MT_MAXR planned ranges; the chunks of range i are
-// stored from state index r[i].first = base + (chunks of earlier ranges).
-// One launch, one block per chunk.
-int mt_prepare_direct(EzMesh *m, uint64_t seed, MtRange *r, int nr, size_t base) {
+// stored from state index r[i].first = base + (chunks of earlier ranges) of
+// `states`, which holds at least base + sum P states.  One launch on `st`,
+// one block per chunk.
+int mt_jump_launch(int dev, cudaStream_t st, uint32_t *states, uint64_t seed,
+    MtRange *r, int nr, size_t base) {
   if (nr > MT_MAXR) return EZMOCK_ERR_UNKNOWN;
   MtJumpArgs a;
   a.nr = nr;
@@ -745,7 +752,7 @@ int mt_prepare_direct(EzMesh *m, uint64_t seed, MtRange *r, int nr, size_t base)
     std::lock_guard<std::mutex> lk(g_mt_mu);
     for (int i = 0; i < nr; i++) {
       r[i].first = base + nst;
-      const uint64_t *d = jump_polys(m->device, r[i].start, r[i].l, (size_t) r[i].P);
+      const uint64_t *d = jump_polys(dev, r[i].start, r[i].l, (size_t) r[i].P);
       if (!d) return EZMOCK_ERR_MEMORY;
       a.P[i] = r[i].P;
       a.first[i] = (uint32_t) r[i].first;
@@ -753,23 +760,58 @@ int mt_prepare_direct(EzMesh *m, uint64_t seed, MtRange *r, int nr, size_t base)
       nst += (size_t) r[i].P;
     }
   }
-  int e = ez_rng_scratch(m, (base + nst) * MT_N * sizeof(uint32_t));
-  if (e) return e;
+  if (!nst) return 0;
   mt_seed_window(seed, a.w);
-  mt_jump_kernel<<<(unsigned) nst, H_THREADS, HJ_SMEM, m->stream>>>(
-      (uint32_t *) m->rng_scratch, a); ez_count_launch();
+  mt_jump_kernel<<<(unsigned) nst, H_THREADS, HJ_SMEM, st>>>(states, a); ez_count_launch();
+  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+}
+
+size_t mt_states_needed(const MtRange *r, int nr, size_t base) {
+  size_t n = base;
+  for (int i = 0; i < nr; i++) n += (size_t) r[i].P;
+  return n;
+}
+
+int mt_prepare_direct(EzMesh *m, uint64_t seed, MtRange *r, int nr, size_t base) {
+  int e = ez_rng_scratch(m, mt_states_needed(r, nr, base) * MT_N * sizeof(uint32_t));
+  if (e) return e;
+  return mt_jump_launch(m->device, m->stream, (uint32_t *) m->rng_scratch, seed, r, nr, base);
+}
+
+// Draws [r.start, r.start + count) from the chunk states of r in `states`.
+int mt_gen_launch(cudaStream_t st, const uint32_t *states, const MtRange &r,
+    uint64_t count, uint32_t *out) {
+  if (!count) return 0;
+  const uint64_t L = 1ULL << r.l;
+  const uint64_t nb = (count + L - 1) / L;
+  if (nb > (uint64_t) r.P) return EZMOCK_ERR_UNKNOWN;
+  mt_ring_kernel<<<(unsigned) nb, R_THREADS, 0, st>>>(states + r.first * MT_N, L, count, out);
+  ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
 int mt_generate(EzMesh *m, const MtRange &r, uint64_t count, uint32_t *out) {
-  if (!count) return 0;
-  const uint32_t *states = (const uint32_t *) m->rng_scratch + r.first * MT_N;
-  const uint64_t L = 1ULL << r.l;
-  const uint64_t nb = (count + L - 1) / L;
-  if (nb > (uint64_t) r.P) return EZMOCK_ERR_UNKNOWN;
-  mt_ring_kernel<<<(unsigned) nb, R_THREADS, 0, m->stream>>>(states, L, count, out);
-  ez_count_launch();
-  return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
+  return mt_gen_launch(m->stream, (const uint32_t *) m->rng_scratch, r, count, out);
+}
+
+// One chunk length for all ranges (generation time is set by the longest
+// chunk): the shortest whose chunks fit the block budget.
+void plan_common(MtRange *r, const uint64_t *starts, const uint64_t *caps, int n) {
+  int l = 12;
+  for (;; l++) {
+    uint64_t tot = 0;
+    for (int i = 0; i < n; i++)
+      tot += (std::max<uint64_t>(caps[i], 1) + (1ULL << l) - 1) >> l;
+    if (tot <= (uint64_t) MT_CHUNKS || l >= 62) break;
+  }
+  for (int i = 0; i < n; i++) {
+    r[i].start = starts[i];
+    r[i].cap = std::max<uint64_t>(caps[i], 1);
+    r[i].l = l;
+    r[i].P = (int) ((r[i].cap + (1ULL << l) - 1) >> l);
+    r[i].p = -1;
+    r[i].first = 0;
+  }
 }
 
 int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
@@ -793,6 +835,24 @@ int mt_fill(EzMesh *m, uint64_t seed, uint64_t start, uint64_t count,
 
 }  // namespace
 
+int ez_rng_fill_around(EzMesh *m, int ran, uint64_t seed, uint64_t start,
+    uint64_t count, uint32_t *out, void (*between)(void *), void *arg) {
+  m->rng_nprep = 0;
+  if (ran == EZMOCK_RNG_MT19937 && count && mt_direct(m->device)) {
+    MtRange r;
+    r.start = start;
+    r.cap = count;
+    plan_direct(r, MT_CHUNKS);
+    int e = mt_prepare_direct(m, seed, &r, 1, 0);
+    if (e) return e;
+    between(arg);
+    return mt_generate(m, r, count, out);
+  }
+  const int e = ez_rng_fill(m, ran, seed, start, count, out);
+  if (!e) between(arg);
+  return e;
+}
+
 int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
     uint64_t count, uint32_t *out) {
   m->rng_nprep = 0;                         // the scratch is reused
@@ -804,44 +864,51 @@ int ez_rng_prepare(EzMesh *m, int ran, uint64_t seed, const uint64_t *starts,
     const uint64_t *caps, int n) {
   m->rng_nprep = 0;
   if (n > EZ_RNG_MAXPREP) return EZMOCK_ERR_UNKNOWN;
+  // ranges the side stream prepared for this seed and generator
+  bool side[EZ_RNG_MAXPREP] = {false, false, false, false};
+  if (m->pre_valid && m->pre_seed == seed && m->pre_ran == ran) {
+    for (int i = 0; i < n && i < m->pre_n; i++)
+      side[i] = m->pre[i].start == starts[i] && m->pre[i].cap >= caps[i];
+    if (side[0] || side[1] || side[2]) {
+      if (!EZ_CUDA_OK(cudaStreamWaitEvent(m->stream, m->ev_side, 0))) return EZMOCK_ERR_UNKNOWN;
+    }
+  }
   for (int i = 0; i < n; i++) {
     m->rng_prep[i].start = starts[i];
     m->rng_prep[i].cap = caps[i];
+    m->rng_prep[i].side = side[i];
+    if (side[i]) {
+      m->rng_prep[i].l = m->pre[i].l;
+      m->rng_prep[i].P = m->pre[i].P;
+      m->rng_prep[i].first = m->pre[i].first;
+    }
   }
   if (ran == EZMOCK_RNG_MT19937) {
+    // the remaining ranges, prepared together on the instance stream
     MtRange r[EZ_RNG_MAXPREP];
-    int e;
-    if (mt_direct(m->device)) {
-      // one chunk length for all ranges (generation time is set by the
-      // longest chunk): the shortest whose chunks fit the block budget
-      int l = 12;
-      for (;; l++) {
-        uint64_t tot = 0;
-        for (int i = 0; i < n; i++)
-          tot += (std::max<uint64_t>(caps[i], 1) + (1ULL << l) - 1) >> l;
-        if (tot <= (uint64_t) MT_CHUNKS || l >= 62) break;
-      }
-      for (int i = 0; i < n; i++) {
-        r[i].start = starts[i];
-        r[i].cap = std::max<uint64_t>(caps[i], 1);
-        r[i].l = l;
-        r[i].P = (int) ((r[i].cap + (1ULL << l) - 1) >> l);
-        r[i].p = -1;
-        r[i].first = 0;
-      }
-      e = mt_prepare_direct(m, seed, r, n, 0);
-    }
-    else {
-      for (int i = 0; i < n; i++) r[i] = mt_plan(starts[i], caps[i] ? caps[i] : 1);
-      e = mt_prepare_ranges(m, seed, r, n, 0);
-    }
-    if (e) return e;
+    uint64_t st2[EZ_RNG_MAXPREP], cp2[EZ_RNG_MAXPREP];
+    int idx[EZ_RNG_MAXPREP], k = 0;
+    for (int i = 0; i < n; i++)
+      if (!side[i]) { idx[k] = i; st2[k] = starts[i]; cp2[k] = caps[i] ? caps[i] : 1; k++; }
     size_t end = 0;
-    for (int i = 0; i < n; i++) {
-      m->rng_prep[i].l = r[i].l;
-      m->rng_prep[i].P = r[i].P;
-      m->rng_prep[i].first = r[i].first;
-      end = std::max(end, r[i].first + (size_t) r[i].P);
+    if (k) {
+      int e;
+      if (mt_direct(m->device)) {
+        plan_common(r, st2, cp2, k);
+        e = mt_prepare_direct(m, seed, r, k, 0);
+      }
+      else {
+        for (int j = 0; j < k; j++) r[j] = mt_plan(st2[j], cp2[j]);
+        e = mt_prepare_ranges(m, seed, r, k, 0);
+      }
+      if (e) return e;
+      for (int j = 0; j < k; j++) {
+        const int i = idx[j];
+        m->rng_prep[i].l = r[j].l;
+        m->rng_prep[i].P = r[j].P;
+        m->rng_prep[i].first = r[j].first;
+        end = std::max(end, r[j].first + (size_t) r[j].P);
+      }
     }
     m->rng_prep_end = end;
   }
@@ -849,15 +916,19 @@ int ez_rng_prepare(EzMesh *m, int ran, uint64_t seed, const uint64_t *starts,
   return 0;
 }
 
-int ez_rng_fill_prepared(EzMesh *m, int ran, uint64_t seed, int i,
-    uint64_t count, uint32_t *out) {
-  if (i >= m->rng_nprep || count > m->rng_prep[i].cap || ran != EZMOCK_RNG_MT19937) {
-    if (ran == EZMOCK_RNG_MT19937)
-      // beyond the prepared capacity: states after the prepared ones
-      return mt_fill(m, seed, m->rng_prep[i < m->rng_nprep ? i : 0].start, count, out,
-          m->rng_nprep ? m->rng_prep_end : 0);
-    return mrg_fill(m, seed, m->rng_prep[i].start, count, out);
+int ez_rng_draws(EzMesh *m, int ran, uint64_t seed, int i, uint64_t count,
+    uint32_t *out, const uint32_t **res) {
+  *res = out;
+  const bool prepared = i < m->rng_nprep && count <= m->rng_prep[i].cap;
+  if (prepared && i == 0 && m->rng_prep[0].side && count <= m->pre_bias_n) {
+    *res = m->draws_bias;                   // generated on the side stream
+    return 0;
   }
+  const uint64_t start = m->rng_prep[i < m->rng_nprep ? i : 0].start;
+  if (ran != EZMOCK_RNG_MT19937) return mrg_fill(m, seed, start, count, out);
+  if (!prepared)
+    // beyond the prepared capacity: states after the prepared ones
+    return mt_fill(m, seed, start, count, out, m->rng_nprep ? m->rng_prep_end : 0);
   MtRange r;
   r.start = m->rng_prep[i].start;
   r.cap = m->rng_prep[i].cap;
@@ -865,7 +936,77 @@ int ez_rng_fill_prepared(EzMesh *m, int ran, uint64_t seed, int i,
   r.P = m->rng_prep[i].P;
   r.p = -1;
   r.first = m->rng_prep[i].first;
-  return mt_generate(m, r, count, out);
+  return mt_gen_launch(m->stream,
+      (const uint32_t *) (m->rng_prep[i].side ? m->rng_side : m->rng_scratch), r, count, out);
+}
+
+void ez_rng_side_prepare(EzMesh *m, int ran, uint64_t seed,
+    const uint64_t *starts, const uint64_t *caps, int n, uint64_t nbias) {
+  m->pre_valid = false;
+  if (n < 1 || n > 3 || !nbias) return;
+  if (ran == EZMOCK_RNG_MT19937 && !mt_direct(m->device)) return;
+  if (!m->side) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);       // lo: lowest priority
+    if (!EZ_CUDA_OK(cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, lo)) ||
+        !EZ_CUDA_OK(cudaEventCreateWithFlags(&m->ev_main, cudaEventDisableTiming)) ||
+        !EZ_CUDA_OK(cudaEventCreateWithFlags(&m->ev_side, cudaEventDisableTiming))) {
+      cudaGetLastError();
+      return;
+    }
+  }
+  if (nbias > m->draws_bias_cap) {
+    if (m->draws_bias) cudaFree(m->draws_bias);
+    m->draws_bias = nullptr;
+    m->draws_bias_cap = 0;
+    if (!EZ_CUDA_OK(cudaMalloc(&m->draws_bias, nbias * sizeof(uint32_t)))) { cudaGetLastError(); return; }
+    m->draws_bias_cap = nbias;
+  }
+  // the side buffers may still be read by earlier work of the instance stream
+  if (!EZ_CUDA_OK(cudaEventRecord(m->ev_main, m->stream)) ||
+      !EZ_CUDA_OK(cudaStreamWaitEvent(m->side, m->ev_main, 0)))
+    return;
+  MtRange r[3];
+  if (ran == EZMOCK_RNG_MT19937) {
+    plan_common(r, starts, caps, n);
+    const size_t need = mt_states_needed(r, n, 0) * MT_N * sizeof(uint32_t);
+    if (need > m->rng_side_cap) {
+      if (m->rng_side) cudaFree(m->rng_side);
+      m->rng_side = nullptr;
+      m->rng_side_cap = 0;
+      if (!EZ_CUDA_OK(cudaMalloc(&m->rng_side, need))) { cudaGetLastError(); return; }
+      m->rng_side_cap = need;
+    }
+    if (mt_jump_launch(m->device, m->side, m->rng_side, seed, r, n, 0) ||
+        mt_gen_launch(m->side, m->rng_side, r[0], std::min<uint64_t>(nbias, r[0].cap),
+            m->draws_bias))
+      return;
+  }
+  else {
+    for (int i = 0; i < n; i++) {
+      r[i].start = starts[i];
+      r[i].cap = caps[i];
+      r[i].l = 0;
+      r[i].P = 0;
+      r[i].first = 0;
+    }
+    n = 1;                                  // MRG32k3a needs no preparation
+    if (mrg_fill_st(m->device, m->side, seed, starts[0], nbias, m->draws_bias)) return;
+  }
+  if (!EZ_CUDA_OK(cudaEventRecord(m->ev_side, m->side))) return;
+  for (int i = 0; i < n; i++) {
+    m->pre[i].start = r[i].start;
+    m->pre[i].cap = r[i].cap;
+    m->pre[i].l = r[i].l;
+    m->pre[i].P = r[i].P;
+    m->pre[i].first = r[i].first;
+    m->pre[i].side = true;
+  }
+  m->pre_n = n;
+  m->pre_ran = ran;
+  m->pre_seed = seed;
+  m->pre_bias_n = std::min<uint64_t>(nbias, r[0].cap);
+  m->pre_valid = true;
 }
 
 // ============================================================================
