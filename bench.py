@@ -211,9 +211,8 @@ def main():
     if args.rng is not None:
         cfg.rng = args.rng
     k, P = bbks_pk()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from ezmock_b200.replicas import Replicas, job_seconds_per_mock, rank_env, rank_seed
+    rank, world, local = rank_env()
     n_gpus = max(world, 1)
 
     if args.impl == "reference":
@@ -236,16 +235,13 @@ def main():
                     "d2h_bytes_per_step": 0}}))
         return 0
 
-    dist = None
     if world > 1:
-        import datetime
         import torch
-        import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    rep = Replicas(world, "nccl")
 
     from ezmock_b200 import EZmock
-    m = EZmock(Lbox=cfg.Lbox, Ngrid=cfg.Ng, rng=cfg.rng, seed=1 + rank * 100000,
+    m = EZmock(Lbox=cfg.Lbox, Ngrid=cfg.Ng, rng=cfg.rng, seed=rank_seed(rank),
                prec=args.prec)
     L = m._L
     m.set_option(3, local)            # device
@@ -257,18 +253,12 @@ def main():
     b = 4 if args.prec == 32 else 8
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        rep.barrier()
 
     def reduce_max(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rep.reduce_max(x, f"cuda:{local}")
 
-    seed = [1 + rank * 100000]
+    seed = [rank_seed(rank)]
 
     def device_step():
         seed[0] += 1
@@ -305,7 +295,7 @@ def main():
     clocks = clk.stop()
     barrier()
     t_dev = reduce_max(ms.value / 1e3)
-    value = t_dev / (n_gpus * args.steps)
+    value = job_seconds_per_mock(t_dev, n_gpus, args.steps)
 
     # end to end through the public API with host buffers
     barrier()
@@ -321,7 +311,7 @@ def main():
     e2e_wall = time.perf_counter() - te0
     ems = ctypes.c_double()
     L.EZmockB200_elapsed(m._ez, 2, 3, ctypes.byref(ems))
-    e2e = reduce_max(max(ems.value / 1e3, e2e_wall)) / (n_gpus * args.steps)
+    e2e = job_seconds_per_mock(reduce_max(max(ems.value / 1e3, e2e_wall)), n_gpus, args.steps)
     h2d = 3 * pk_trim_len(k, cfg.Ng, cfg.Lbox) * 8
     d2h = 6 * len(cat[0]) * b
 
@@ -365,9 +355,8 @@ def main():
                                     "kind": "reference", "sample": f"unavailable: {e}"}
     if rank == 0:
         print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.barrier()
+    rep.close()
     return 0
 
 
