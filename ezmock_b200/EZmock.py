@@ -205,3 +205,54 @@ class EZmock:
 
     def sync(self):
         return self._L.EZmockB200_sync(self._ez)
+
+    def _cat_args(self, cat):
+        """(x, y, z, vz, n, keep-alive) for host arrays, or NULLs for the
+        instance's last catalogue on the GPU."""
+        if cat is None:
+            return None, None, None, None, 0, None
+        arrs = [np.ascontiguousarray(np.asarray(a), dtype=self._rdt) for a in cat]
+        if len(arrs) not in (3, 4) or any(a.ndim != 1 or a.shape != arrs[0].shape for a in arrs):
+            raise ValueError("catalogue: x, y, z[, vz] as 1d arrays of equal length")
+        ptrs = [a.ctypes.data_as(ctypes.c_void_p) for a in arrs]
+        if len(ptrs) == 3:
+            ptrs.append(None)
+        return ptrs[0], ptrs[1], ptrs[2], ptrs[3], arrs[0].shape[0], arrs
+
+    def powspec(self, cat=None, rsd_fac=0.0, ngrid=256, interlace=True, kmin=0.0,
+                kmax=0.3, nbin=30):
+        """Power-spectrum multipoles of the last catalogue (cat=None, kept on
+        the GPU) or of host arrays cat = (x, y, z[, vz]).  Returns a dict of
+        k_mean, nmodes, P0, P2 (arrays of nbin)."""
+        x, y, z, vz, n, keep = self._cat_args(cat)
+        out = [np.zeros(int(nbin)) for _ in range(4)]
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._err.value = self._L.EZmockB200_powspec(
+            self._ez, x, y, z, vz, n, float(rsd_fac), int(ngrid), int(bool(interlace)),
+            float(kmin), float(kmax), int(nbin), *[o.ctypes.data_as(dp) for o in out],
+            ctypes.byref(self._err))
+        del keep
+        self._assert_return_value()
+        return dict(zip(("k_mean", "nmodes", "P0", "P2"), out))
+
+    def cic_pdf(self, cat=None, rsd_fac=0.0, ngrid=64, nbin=32):
+        """Fraction of the ngrid^3 cells holding c = 0 .. nbin-2 tracers, and
+        at least nbin-1 tracers in the last bin."""
+        x, y, z, vz, n, keep = self._cat_args(cat)
+        out = np.zeros(int(nbin))
+        self._err.value = self._L.EZmockB200_cic_pdf(
+            self._ez, x, y, z, vz, n, float(rsd_fac), int(ngrid), int(nbin),
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(self._err))
+        del keep
+        self._assert_return_value()
+        return out
+
+
+def powspec_table(res, kmin=0.0, kmax=0.3):
+    """Rows in the column order the reference's plotting reads
+    (example/fit/pyclustering.py:249-251: k in column 0, P0 in 5, P2 in 6):
+    k_center, k_low, k_high, k_mean, nmodes, P0, P2."""
+    nb = len(res["P0"])
+    edges = np.linspace(kmin, kmax, nb + 1)
+    return np.column_stack([0.5 * (edges[:-1] + edges[1:]), edges[:-1], edges[1:],
+                            res["k_mean"], res["nmodes"], res["P0"], res["P2"]])

@@ -81,6 +81,14 @@ def load(prec=32):
     L.EZmockB200_mt19937_fill_noalloc.restype = ctypes.c_int
     L.EZmockB200_mt19937_fill_noalloc.argtypes = [ctypes.c_uint64, ctypes.c_uint64,
                                                   ctypes.c_uint64, _vp, _vp]
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.EZmockB200_powspec.restype = ctypes.c_int
+    L.EZmockB200_powspec.argtypes = [_vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_double,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, _ip]
+    L.EZmockB200_cic_pdf.restype = ctypes.c_int
+    L.EZmockB200_cic_pdf.argtypes = [_vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, ctypes.c_double,
+                                     ctypes.c_int, ctypes.c_int, dp, _ip]
     L.EZmockB200_sync.restype = ctypes.c_int
     L.EZmockB200_sync.argtypes = [_vp]
     L.EZmockB200_real_size.restype = ctypes.c_int

@@ -897,11 +897,18 @@ int ez_fft_c2r_psi(EzMesh *m) {
 // r2c(delta) (sign -1, unnormalised) into spec[0]
 // (libEZmock/EZmock/dens_field.c:195-201).
 int ez_fft_r2c_delta(EzMesh *m, const real *d_delta) {
-  const int Ng = m->Ng, Nkp = m->Nkp, Nh = Ng / 2;
+  return ez_fft_r2c(m->device, m->stream, d_delta, m->spec[0], m->Ng, m->Nkp);
+}
+
+// Forward (sign -1, unnormalised) r2c of an Ng^3 real grid into half-complex
+// rows of Nkp >= Ng/2 + 1 values (FFTW's r2c layout, padded).
+int ez_fft_r2c(int dev, cudaStream_t st, const real *in, cplx *out, int Ng, int Nkp) {
+  const int Nh = Ng / 2;
+  const int Nk = Nh + 1;
   FftPlanDev pn, ph;
-  if (!make_plan(m->device, Ng, &pn) || !make_plan(m->device, Nh, &ph))
+  if (!make_plan(dev, Ng, &pn) || !make_plan(dev, Nh, &ph))
     return EZMOCK_ERR_UNKNOWN;
-  const cplx *twg = twiddles(m->device, Ng);
+  const cplx *twg = twiddles(dev, Ng);
   if (!twg) return EZMOCK_ERR_UNKNOWN;
   int R = 8;
   while (R > 1 && sizeof(cplx) * (2 * (size_t) Nh + 1 + 2 * (size_t) Nh * R) > 160 * 1024) R >>= 1;
@@ -915,11 +922,11 @@ int ez_fft_r2c_delta(EzMesh *m, const real *d_delta) {
     attr_done = 1;
   }
   const size_t nrows = (size_t) Ng * Ng;
-  fft_r2c_rows<<<(unsigned) ((nrows + R - 1) / R), FFT_NT, sm_r, m->stream>>>(
-      d_delta, m->spec[0], Ng, Nkp, R, nrows, ph, twg); ez_count_launch();
-  const int nkt = (m->Nk + K - 1) / K;
-  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, m->stream>>>(m->spec[0], Ng, Nkp, K, 1, pn); ez_count_launch();
-  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, m->stream>>>(m->spec[0], Ng, Nkp, K, 0, pn); ez_count_launch();
+  fft_r2c_rows<<<(unsigned) ((nrows + R - 1) / R), FFT_NT, sm_r, st>>>(
+      in, out, Ng, Nkp, R, nrows, ph, twg); ez_count_launch();
+  const int nkt = (Nk + K - 1) / K;
+  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, st>>>(out, Ng, Nkp, K, 1, pn); ez_count_launch();
+  fft_axis_one<-1><<<dim3(Ng, nkt), FFT_NT, sm_a, st>>>(out, Ng, Nkp, K, 0, pn); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 

@@ -150,6 +150,7 @@ void mesh_free_device(EzMesh *m) {
   if (m->rng_scratch) cudaFree(m->rng_scratch);
   if (m->fixacc) cudaFree(m->fixacc);
   if (m->pkq) cudaFree(m->pkq);
+  if (m->est) cudaFree(m->est);
   if (m->stats) cudaFree(m->stats);
   if (m->cat) cudaFree(m->cat);
   if (m->h_stage) cudaFreeHost(m->h_stage);
@@ -960,6 +961,52 @@ int EZmockB200_rng_raw(const int randgen, const uint64_t seed,
   if (m.rng_scratch) cudaFree(m.rng_scratch);
   cudaStreamDestroy(m.stream);
   return e;
+}
+
+// Device and stream of an instance that has no field yet.
+int ensure_stream(EzMesh *m) {
+  if (m->device < 0 && !EZ_CUDA_OK(cudaGetDevice(&m->device))) {
+    cudaGetLastError();
+    m->device = -1;
+    return EZMOCK_ERR_UNKNOWN;
+  }
+  if (set_device(m)) return EZMOCK_ERR_UNKNOWN;
+  if (!m->stream) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (!EZ_CUDA_OK(cudaStreamCreateWithPriority(&m->stream, cudaStreamNonBlocking, hi)))
+      return EZMOCK_ERR_UNKNOWN;
+  }
+  return 0;
+}
+
+int EZmockB200_powspec(EZMOCK *ez, const real *x, const real *y, const real *z,
+    const real *vz, const size_t n, const double rsd_fac, const int ngrid,
+    const int interlace, const double kmin, const double kmax, const int nbin,
+    double *kavg, double *nmodes, double *pk0, double *pk2, int *err) {
+  if (!err) return EZMOCK_ERR_ARG_ECODE;
+  if (*err != EZMOCK_SUCCESS) return *err;
+  if (!ez) return (*err = EZMOCK_ERR_ARG_EZ);
+  if (!kavg || !nmodes || !pk0 || !pk2) return (*err = EZMOCK_ERR_ARG_NULL);
+  if (x && !n) return (*err = EZMOCK_ERR_ARG_NDATA);
+  EzMesh *m = MESH(ez);
+  int e = ensure_stream(m);
+  if (!e) e = ez_powspec(m, CONF(ez)->Lbox, x, y, z, vz, n, rsd_fac, ngrid, interlace ? 1 : 0,
+      kmin, kmax, nbin, kavg, nmodes, pk0, pk2);
+  return (*err = e);
+}
+
+int EZmockB200_cic_pdf(EZMOCK *ez, const real *x, const real *y, const real *z,
+    const real *vz, const size_t n, const double rsd_fac, const int ngrid,
+    const int nbin, double *pdf, int *err) {
+  if (!err) return EZMOCK_ERR_ARG_ECODE;
+  if (*err != EZMOCK_SUCCESS) return *err;
+  if (!ez) return (*err = EZMOCK_ERR_ARG_EZ);
+  if (!pdf) return (*err = EZMOCK_ERR_ARG_NULL);
+  EzMesh *m = MESH(ez);
+  int e = ensure_stream(m);
+  if (!e) e = ez_cic_pdf(m, CONF(ez)->Lbox, x, y, z, vz, n, rsd_fac, ngrid, nbin, pdf);
+  return (*err = e);
 }
 
 int EZmockB200_sync(EZMOCK *ez) {

@@ -115,6 +115,8 @@ struct EzMesh {
   uint64_t pre_seed, pre_bias_n;
   EzRange pre[3];
   size_t pop_hint;         // tracer capacity of the last population (0: none)
+  void *est;               // clustering-estimator buffer (ez_pk.cu)
+  size_t est_cap;
   unsigned long long *fixacc;   // deterministic CIC accumulators (4 x N)
   double *pkq;             // interpolated P(k) by integer k^2 (3 (Ng/2)^2 + 1)
   void *stats;             // EzCicStats on the device
@@ -138,6 +140,21 @@ struct EzCicStats {
 
 // ---- error helpers ----
 #define EZ_CUDA_OK(call) (cudaSuccess == (call))
+
+// ---- FFT (ez_fft.cu) ----
+// Forward (sign -1, unnormalised) r2c of an Ng^3 real grid into half-complex
+// rows padded to Nkp values; Ng as accepted by ez_fft_supported.
+int ez_fft_r2c(int dev, cudaStream_t st, const real *in, cplx *out, int Ng, int Nkp);
+bool ez_fft_supported(int Ng);
+
+// ---- clustering estimators (ez_pk.cu) ----
+// Catalogue: the instance's last catalogue on the device (x == NULL) or host
+// arrays of n tracers (vz may be NULL: no redshift-space shift).
+int ez_powspec(EzMesh *m, double L, const real *x, const real *y, const real *z,
+    const real *vz, size_t n, double rsd, int Ng, int interlace, double kmin,
+    double kmax, int nbin, double *kavg, double *nmodes, double *p0, double *p2);
+int ez_cic_pdf(EzMesh *m, double L, const real *x, const real *y, const real *z,
+    const real *vz, size_t n, double rsd, int Ng, int nbin, double *pdf);
 
 // ---- RNG (ez_rng.cu) ----
 // Raw 32-bit draws [start, start+count) of the stream seeded by `seed`.

@@ -82,6 +82,30 @@ int EZmockB200_rng_raw(const int randgen, const uint64_t seed,
 int EZmockB200_mt19937_fill_noalloc(const uint64_t seed, const uint64_t start,
     const uint64_t count, uint32_t *d_out, void *stream);
 
+/* Clustering of a catalogue in the instance's periodic box (no counterpart
+   in libEZmock: the reference calls external programs,
+   example/fit/pyclustering.py:173-186, with example/fit/conf/powspec.conf).
+   Catalogue: x == NULL selects the instance's last catalogue, kept on the
+   GPU; otherwise x, y, z (and vz, may be NULL) are host arrays of n tracers.
+   With vz and rsd_fac != 0 the z coordinate is moved to redshift space,
+   z + rsd_fac vz wrapped into [0, Lbox).
+
+   EZmockB200_powspec: power-spectrum multipoles l = 0, 2 with CIC assignment
+   on ngrid^3 (even, 5-smooth), optional interlacing, window compensation,
+   line of sight z, nbin linear bins of |k| in [kmin, kmax) h/Mpc; per bin the
+   mean |k|, the number of modes, P0 (shot noise Lbox^3/N subtracted) and P2
+   in (Mpc/h)^3.
+
+   EZmockB200_cic_pdf: fraction of the ngrid^3 cells holding c tracers,
+   c = 0 .. nbin-2, and c >= nbin-1 in the last bin (nbin <= 1024). */
+int EZmockB200_powspec(EZMOCK *ez, const real *x, const real *y, const real *z,
+    const real *vz, const size_t n, const double rsd_fac, const int ngrid,
+    const int interlace, const double kmin, const double kmax, const int nbin,
+    double *kavg, double *nmodes, double *pk0, double *pk2, int *err);
+int EZmockB200_cic_pdf(EZMOCK *ez, const real *x, const real *y, const real *z,
+    const real *vz, const size_t n, const double rsd_fac, const int ngrid,
+    const int nbin, double *pdf, int *err);
+
 /* Waits for all work of the instance. */
 int EZmockB200_sync(EZMOCK *ez);
 
