@@ -34,7 +34,7 @@ enum {
   E_PK_NONPOS = 22, E_PK_NONASC = 23, E_PK_RANGE = 24, E_PK_NBIN = 25,
   E_PK_MODBAO = 26, E_RNG_JUMP = 29, E_PAR_COSMO = 30, E_PAR_RCUT = 31,
   E_PAR_REXP = 32, E_PAR_PBASE = 33, E_PAR_SIGV = 34, E_RHO_LESS = 36,
-  E_RHO_PBASE = 37, E_UNKNOWN = 41
+  E_RHO_PBASE = 37, E_RHO_NPART = 38, E_UNKNOWN = 41
 };
 
 #define NLOGB 64          /* config.h:64 */
@@ -755,10 +755,97 @@ void ezo_rsd(size_t n, const real *z, const real *vz, double rsd_fac,
   }
 }
 
-/* EZmock_populate_tracer (pop_tracer.c:1140-1219), att_part = false. */
+/* Eulerian position of particle (i,j,k) in grid units, wrapped into
+   [0, Ng), and its nearest grid cell (pop_tracer.c:541-561, :819-835). */
+static size_t ngp_cell(int Ng, real igs, const real *psi0, const real *psi1,
+    const real *psi2, int i, int j, int k, real *p) {
+  const size_t idx = IDX3(Ng, i, j, k);
+  real px = psi0[idx] * igs + i;
+  real py = psi1[idx] * igs + j;
+  real pz = psi2[idx] * igs + k;
+  if (px < 0) px += Ng;
+  else if (px >= Ng) px -= Ng;
+  if (py < 0) py += Ng;
+  else if (py >= Ng) py -= Ng;
+  if (pz < 0) pz += Ng;
+  else if (pz >= Ng) pz -= Ng;
+  int ix = (int) (px + 0.5);
+  int iy = (int) (py + 0.5);
+  int iz = (int) (pz + 0.5);
+  if (ix >= Ng) ix = 0;
+  if (iy >= Ng) iy = 0;
+  if (iz >= Ng) iz = 0;
+  p[0] = px; p[1] = py; p[2] = pz;
+  return IDX3(Ng, ix, iy, iz);
+}
+
+/* Particles per tracer-hosting cell (pop_tracer.c:517-582). */
+int ezo_count_particles(int Ng, double Lbox, const real *psi0, const real *psi1,
+    const real *psi2, const int16_t *nt, uint16_t *np) {
+  const real igs = Ng / Lbox;
+  memset(np, 0, sizeof(uint16_t) * (size_t) Ng * Ng * Ng);
+  real p[3];
+  for (int i = 0; i < Ng; i++)
+    for (int j = 0; j < Ng; j++)
+      for (int k = 0; k < Ng; k++) {
+        const size_t c = ngp_cell(Ng, igs, psi0, psi1, psi2, i, j, k, p);
+        if (nt[c] == 0) continue;
+        if (np[c] == UINT16_MAX) return E_RHO_NPART;
+        np[c]++;
+      }
+  return E_OK;
+}
+
+/* Tracers attached to particles (pop_tracer.c:804-879): particles in index
+   order; in a cell with fewer tracers than particles each particle takes one
+   draw of the stream from 4N and is kept if u np < nt (selection sampling).
+   nt and np are consumed; *iv = number of attached tracers. */
+int ezo_attach(int Ng, double Lbox, int rng, uint64_t seed, double vfac,
+    const real *psi0, const real *psi1, const real *psi2, int16_t *nt,
+    uint16_t *np, size_t ntot, real *x, real *y, real *z, real *vx, real *vy,
+    real *vz, size_t *iv) {
+  const size_t num = (size_t) Ng * Ng * Ng;
+  const real igs = Ng / Lbox, gs = Lbox / Ng;
+  uint32_t *u = malloc(sizeof(uint32_t) * num);
+  if (!u) return E_MEMORY;
+  rng_fill(rng, seed, num << 2, num, u);
+  size_t cnt = 0, d = 0;
+  real p[3];
+  for (int i = 0; i < Ng; i++)
+    for (int j = 0; j < Ng; j++)
+      for (int k = 0; k < Ng; k++) {
+        const size_t c = ngp_cell(Ng, igs, psi0, psi1, psi2, i, j, k, p);
+        if (nt[c] == 0) continue;
+        if (nt[c] < np[c]) {
+          const double ran = u_dbl(rng, u[d++]);
+          if (ran * np[c] >= nt[c]) {
+            np[c]--;
+            continue;
+          }
+        }
+        nt[c]--;
+        np[c]--;
+        if (cnt >= ntot) { free(u); return E_UNKNOWN; }
+        const size_t id = IDX3(Ng, i, j, k);
+        x[cnt] = p[0] * gs;
+        y[cnt] = p[1] * gs;
+        z[cnt] = p[2] * gs;
+        vx[cnt] = psi0[id] * vfac;
+        vy[cnt] = psi1[id] * vfac;
+        vz[cnt] = psi2[id] * vfac;
+        cnt++;
+      }
+  free(u);
+  *iv = cnt;
+  return E_OK;
+}
+
+/* EZmock_populate_tracer (pop_tracer.c:1140-1219).  With att_part the
+   attached tracers come first, the others follow in cell order (the OpenMP
+   build's layout, pop_tracer.c:916-931). */
 int ezo_populate(int Ng, double Lbox, int rng, uint64_t seed, double vfac,
     const real *psi0, const real *psi1, const real *psi2, const real *rho,
-    const real *params, size_t nexp, size_t cap, size_t *ntracer,
+    const real *params, size_t nexp, int att_part, size_t cap, size_t *ntracer,
     real *x, real *y, real *z, real *vx, real *vy, real *vz) {
   const size_t num = (size_t) Ng * Ng * Ng;
   if (nexp < 128) return E_ARG_LOWEXP;
@@ -784,14 +871,25 @@ int ezo_populate(int Ng, double Lbox, int rng, uint64_t seed, double vfac,
   }
   free(rhot);
   if (ntot > cap) { free(nt); free(paint); *ntracer = ntot; return E_MEMORY; }
-  if ((e = ezo_positions(Ng, Lbox, rng, seed, nt, ntot, x, y, z))) {
+  size_t iv = 0;
+  if (att_part) {
+    uint16_t *np = malloc(sizeof(uint16_t) * num);
+    if (!np) { free(nt); free(paint); return E_MEMORY; }
+    if ((e = ezo_count_particles(Ng, Lbox, psi0, psi1, psi2, nt, np)) ||
+        (e = ezo_attach(Ng, Lbox, rng, seed, vfac, psi0, psi1, psi2, nt, np, ntot,
+            x, y, z, vx, vy, vz, &iv))) {
+      free(np); free(nt); free(paint); return e;
+    }
+    free(np);
+  }
+  if ((e = ezo_positions(Ng, Lbox, rng, seed, nt, ntot - iv, x + iv, y + iv, z + iv))) {
     free(nt); free(paint); return e;
   }
   free(nt);
   for (int d = 0; d < 3; d++) {
     ezo_paint(Ng, Lbox, psi0, psi1, psi2, rho, d, paint);
-    ezo_assign_vel(Ng, Lbox, vfac, paint, rho, ntot, x, y, z,
-        (d == 0) ? vx : (d == 1) ? vy : vz);
+    ezo_assign_vel(Ng, Lbox, vfac, paint, rho, ntot - iv, x + iv, y + iv, z + iv,
+        ((d == 0) ? vx : (d == 1) ? vy : vz) + iv);
   }
   free(paint);
   ezo_vel_scatter(Ng, rng, seed, ntot, sigma_v, vx, vy, vz);

@@ -85,11 +85,21 @@ void ezo_vel_scatter(int Ng, int rng, uint64_t seed, size_t n, real sigma_v,
 void ezo_rsd(size_t n, const real *z, const real *vz, double rsd_fac,
     double Lbox, double *zout);
 
-/* Whole EZmock_populate_tracer (pop_tracer.c:1140-1219, att_part = false).
+/* pop_tracer.c:517-582: particles per tracer-hosting cell (nearest cell). */
+int ezo_count_particles(int Ng, double Lbox, const real *psi0, const real *psi1,
+    const real *psi2, const int16_t *nt, uint16_t *np);
+/* pop_tracer.c:804-879: tracers attached to particles (serial selection
+   sampling, draws from 4N); consumes nt and np. */
+int ezo_attach(int Ng, double Lbox, int rng, uint64_t seed, double vfac,
+    const real *psi0, const real *psi1, const real *psi2, int16_t *nt,
+    uint16_t *np, size_t ntot, real *x, real *y, real *z, real *vx, real *vy,
+    real *vz, size_t *iv);
+
+/* Whole EZmock_populate_tracer (pop_tracer.c:1140-1219).
    Arrays x..vz must hold `cap` entries; returns 0 or an EZmock error code. */
 int ezo_populate(int Ng, double Lbox, int rng, uint64_t seed, double vfac,
     const real *psi0, const real *psi1, const real *psi2, const real *rho,
-    const real *params, size_t nexp, size_t cap, size_t *ntracer,
+    const real *params, size_t nexp, int att_part, size_t cap, size_t *ntracer,
     real *x, real *y, real *z, real *vx, real *vy, real *vz);
 
 /* Raw 32-bit draws of a stream (for RNG parity tests). */

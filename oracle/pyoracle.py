@@ -86,8 +86,8 @@ class Oracle:
         L.ezo_rsd.argtypes = [ctypes.c_size_t, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]
         L.ezo_populate.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_uint64, ctypes.c_double, _vp, _vp, _vp, _vp,
-                                   _vp, ctypes.c_size_t, ctypes.c_size_t, _c_size_p,
-                                   _vp, _vp, _vp, _vp, _vp, _vp]
+                                   _vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_size_t,
+                                   _c_size_p, _vp, _vp, _vp, _vp, _vp, _vp]
         L.ezo_rng_raw.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
                                   ctypes.c_uint64, _vp]
 
@@ -202,7 +202,8 @@ class Oracle:
                          _ptr(np.ascontiguousarray(vz, self.rdt)), rsd_fac, Lbox, _ptr(out))
         return out
 
-    def populate(self, Ng, Lbox, rng, seed, vfac, psi, rho, params, nexp, cap=None):
+    def populate(self, Ng, Lbox, rng, seed, vfac, psi, rho, params, nexp, cap=None,
+                 att_part=False):
         if cap is None:
             cap = 4 * nexp + 1024
         prm = np.array(params, self.rdt)
@@ -211,7 +212,8 @@ class Oracle:
         psi = [np.ascontiguousarray(p, self.rdt) for p in psi]
         e = self.lib.ezo_populate(Ng, Lbox, rng, seed, vfac, *[_ptr(p) for p in psi],
                                   _ptr(np.ascontiguousarray(rho, self.rdt)), _ptr(prm), nexp,
-                                  cap, ctypes.byref(n), *[_ptr(c) for c in cat])
+                                  int(bool(att_part)), cap, ctypes.byref(n),
+                                  *[_ptr(c) for c in cat])
         if e:
             return e, None
         return 0, [c[:n.value].copy() for c in cat]
@@ -342,11 +344,12 @@ class _RefMock:
         self._chk()
         return nt.reshape((self.Ng,) * 3), pdf_out, nc.value, no.value
 
-    def populate(self, params, nexp):
+    def populate(self, params, nexp, att_part=False):
         prm = np.array(params, self.o.rdt)
         n = ctypes.c_size_t()
         ptrs = [_vp() for _ in range(6)]
-        self.o.lib.EZmock_populate_tracer(self.ez, _ptr(prm), nexp, False, ctypes.byref(n),
+        self.o.lib.EZmock_populate_tracer(self.ez, _ptr(prm), nexp, bool(att_part),
+                                          ctypes.byref(n),
                                           *[ctypes.byref(p) for p in ptrs],
                                           ctypes.byref(self.err))
         self._chk()

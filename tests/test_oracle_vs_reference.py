@@ -83,6 +83,29 @@ def test_populate_bitexact(pk_table, prec, rng, params, n):
 
 
 @pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("rng", [0, 1])
+@pytest.mark.parametrize("params,n", [([0.6, 15.0, 0.35, 300.0], 3e-4),
+                                      ([1.2, 5.0, 0.2, 150.0], 1e-4),
+                                      ([0.0, 10.0, 0.3, 0.0], 2e-3)])
+def test_populate_attached_to_particles(pk_table, prec, rng, params, n):
+    """att_part = true: tracers attached to particles by the serial
+    selection-sampling chain (pop_tracer.c:517-582, :804-879)."""
+    k, P = pk_table
+    Ng, L = 32, 250.0
+    R, O, m, t, vf = _pair(prec, Ng, L, rng, 2, k, P)
+    m.create()
+    nexp = int(n * L ** 3)
+    cat_r = m.populate(params, nexp, att_part=True)
+    psi, rho = O.dens_field(t, Ng, L, rng, 2)
+    e, cat_o = O.populate(Ng, L, rng, 2, vf, psi, rho, params, nexp, att_part=True)
+    assert e == 0
+    for a, b in zip(cat_r, cat_o):
+        assert np.array_equal(a, b)
+    e, plain = O.populate(Ng, L, rng, 2, vf, psi, rho, params, nexp)
+    assert len(plain[0]) == len(cat_o[0]) and not np.array_equal(plain[0], cat_o[0])
+
+
+@pytest.mark.parametrize("prec", [64, 32])
 def test_multithreaded_reference_counts(pk_table, prec):
     """Eight OpenMP threads: atomic CIC order changes rho by rounding only,
     and every per-cell tracer count is unchanged."""
