@@ -151,6 +151,7 @@ void mesh_free_device(EzMesh *m) {
   if (m->fixacc) cudaFree(m->fixacc);
   if (m->pkq) cudaFree(m->pkq);
   if (m->est) cudaFree(m->est);
+  if (m->att) cudaFree(m->att);
   if (m->stats) cudaFree(m->stats);
   if (m->cat) cudaFree(m->cat);
   if (m->h_stage) cudaFreeHost(m->h_stage);
@@ -244,9 +245,6 @@ int run_populate(EZMOCK *ez, const real *params, size_t nexp, bool att_part,
   if (!std::isfinite(rho_exp) || rho_exp <= 0) return (*err = EZMOCK_ERR_PAR_REXP);
   if (!std::isfinite(pbase) || pbase <= 0 || pbase >= 1) return (*err = EZMOCK_ERR_PAR_PBASE);
   if (!std::isfinite(sigma_v) || sigma_v < 0) return (*err = EZMOCK_ERR_PAR_SIGV);
-  // Attaching tracers to particles is a serial draw chain in the reference
-  // (pop_tracer.c:804-879) and is not provided by this engine.
-  if (att_part) return (*err = EZMOCK_ERR_UNKNOWN);
 
   std::vector<size_t> pdf;
   int nmax;
@@ -256,7 +254,7 @@ int run_populate(EZMOCK *ez, const real *params, size_t nexp, bool att_part,
   if ((e = set_device(m))) return (*err = e);
   EzPopResult res;
   e = ez_populate(m, conf->Ng, conf->Lbox, RNG(ez)->ran, RNG(ez)->seed,
-      COSMO(ez)->vfac, params, pdf.data(), nmax, ncell, ntot, &res);
+      COSMO(ez)->vfac, params, pdf.data(), nmax, ncell, ntot, att_part, &res);
   if (e) return (*err = e);
   if (res.err) return (*err = res.err);
   *ntracer = res.ntot;

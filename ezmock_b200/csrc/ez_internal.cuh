@@ -117,6 +117,8 @@ struct EzMesh {
   size_t pop_hint;         // tracer capacity of the last population (0: none)
   void *est;               // clustering-estimator buffer (ez_pk.cu)
   size_t est_cap;
+  void *att;               // attach-to-particle stage buffer (ez_pop.cu)
+  size_t att_cap;
   unsigned long long *fixacc;   // deterministic CIC accumulators (4 x N)
   double *pkq;             // interpolated P(k) by integer k^2 (3 (Ng/2)^2 + 1)
   void *stats;             // EzCicStats on the device
@@ -165,6 +167,9 @@ int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
 // generation), so that work launched there can share the SMs with it.
 int ez_rng_fill_around(EzMesh *m, int ran, uint64_t seed, uint64_t start,
     uint64_t count, uint32_t *out, void (*between)(void *), void *arg);
+// ez_rng_fill that keeps the prepared ranges (their states stay valid).
+int ez_rng_fill_free(EzMesh *m, int ran, uint64_t seed, uint64_t start,
+    uint64_t count, uint32_t *out);
 // Prepares the ranges [starts[i], starts[i] + caps[i]) of one stream so that
 // later fills of them skip the jump (MT19937 chunk states computed together).
 #define EZ_RNG_MAXPREP 4
@@ -207,7 +212,7 @@ struct EzPopResult {
 };
 int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
     double vfac, const real *params, const size_t *pdf, int nmax,
-    size_t ncell, size_t ntot, EzPopResult *res);
+    size_t ncell, size_t ntot, bool att_part, EzPopResult *res);
 
 // Counts kernel launches made by the library (reported to benchmarks).
 void ez_count_launch();

@@ -398,7 +398,8 @@ __device__ __forceinline__ int cell_count(real v, const real *lo, const int *ntr
 
 __global__ void __launch_bounds__(NT)
 tracer_count_kernel(const real *__restrict__ rhot, size_t N,
-    const BoundOut *__restrict__ bo, unsigned long long *cnt) {
+    const BoundOut *__restrict__ bo, unsigned long long *cnt,
+    const int16_t *__restrict__ nt16) {
   __shared__ real slo[EZ_MAX_NT];
   __shared__ int sntr[EZ_MAX_NT];
   __shared__ unsigned long long sw[32];
@@ -411,12 +412,12 @@ tracer_count_kernel(const real *__restrict__ rhot, size_t N,
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {               // all loads first
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    v[q] = (id < N) ? rhot[id] : (real) 0;
+    v[q] = (id < N && !nt16) ? rhot[id] : (real) 0;
   }
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    if (id < N) c += cell_count(v[q], slo, sntr, nb);
+    if (id < N) c += nt16 ? nt16[id] : cell_count(v[q], slo, sntr, nb);
   }
   unsigned long long tot;
   block_scan<unsigned long long>(c, &tot, sw);
@@ -446,7 +447,7 @@ template <typename cid_t>
 __global__ void __launch_bounds__(NT)
 tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
     const BoundOut *__restrict__ bo, const unsigned long long *__restrict__ off,
-    unsigned long long ntr, cid_t *__restrict__ cid) {
+    unsigned long long ntr, cid_t *__restrict__ cid, const int16_t *__restrict__ nt16) {
   constexpr int NW = NT / 32;
   __shared__ real slo[EZ_MAX_NT];
   __shared__ int sntr[EZ_MAX_NT];
@@ -463,12 +464,12 @@ tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {               // all loads first
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    v[q] = (id < N) ? rhot[id] : (real) 0;
+    v[q] = (id < N && !nt16) ? rhot[id] : (real) 0;
   }
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    n[q] = (id < N) ? cell_count(v[q], slo, sntr, nb) : 0;
+    n[q] = (id < N) ? (nt16 ? (int) nt16[id] : cell_count(v[q], slo, sntr, nb)) : 0;
     unsigned int incl = (unsigned int) n[q];
     if (__ballot_sync(0xffffffffu, n[q] != 0)) {
 #pragma unroll
@@ -533,6 +534,296 @@ place_kernel(const cid_t *__restrict__ cid, unsigned long long ntr, int Ng,
     if (yy < 0) yy = (double) yy + Lbox;
     if (zz < 0) zz = (double) zz + Lbox;
     x[t] = xx; y[t] = yy; z[t] = zz;
+  }
+}
+
+// ============================================================================
+//     tracers attached to particles (att_part; pop_tracer.c:517-582, :804-879)
+// ============================================================================
+// Particle ids are 32-bit here (Ng^3 < 2^32).
+
+// Eulerian position (grid units, wrapped into [0, Ng)) and nearest cell of
+// particle id, in the reference's `real` arithmetic (pop_tracer.c:541-561).
+__device__ __forceinline__ uint32_t ngp_of(const real *__restrict__ p0,
+    const real *__restrict__ p1, const real *__restrict__ p2, uint32_t id,
+    int Ng, real igs, real *pos) {
+  const uint32_t ij = id / (uint32_t) Ng, i = ij / (uint32_t) Ng;
+  const int k = (int) (id - ij * Ng), j = (int) (ij - i * Ng);
+  real px = p0[id] * igs + (int) i;
+  real py = p1[id] * igs + j;
+  real pz = p2[id] * igs + k;
+  if (px < 0) px += Ng;
+  else if (px >= Ng) px -= Ng;
+  if (py < 0) py += Ng;
+  else if (py >= Ng) py -= Ng;
+  if (pz < 0) pz += Ng;
+  else if (pz >= Ng) pz -= Ng;
+  int ix = (int) ((double) px + 0.5), iy = (int) ((double) py + 0.5),
+      iz = (int) ((double) pz + 0.5);
+  if (ix >= Ng) ix = 0;
+  if (iy >= Ng) iy = 0;
+  if (iz >= Ng) iz = 0;
+  pos[0] = px; pos[1] = py; pos[2] = pz;
+  return ((uint32_t) ix * Ng + iy) * Ng + iz;
+}
+
+// Particles per tracer-hosting cell.
+__global__ void __launch_bounds__(NT)
+np_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
+    const real *__restrict__ p2, uint32_t N, int Ng, real igs,
+    const int16_t *__restrict__ nt, unsigned int *np) {
+  real pos[3];
+  for (uint32_t id = blockIdx.x * NT + threadIdx.x; id < N; id += gridDim.x * NT) {
+    const uint32_t c = ngp_of(p0, p1, p2, id, Ng, igs, pos);
+    if (nt[c] > 0) atomicAdd(np + c, 1u);
+  }
+}
+
+// Exclusive ranks, in index order, of the flagged cells of a chunk of ROWS x
+// NT cells (row q, thread t: cell q NT + t), and the chunk total.
+constexpr int NWP = NT / 32;
+__device__ __forceinline__ unsigned int chunk_ranks(const bool *f, unsigned int *rk,
+    unsigned int *pre, unsigned int *wsum) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned int lt = (1u << lane) - 1;
+  unsigned int bal[ROWS];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    bal[q] = __ballot_sync(0xffffffffu, f[q]);
+    if (lane == 0) pre[q * NWP + w] = __popc(bal[q]);
+  }
+  __syncthreads();
+  unsigned int c = 0, incl = 0;
+  if (threadIdx.x < ROWS * NWP) {
+    c = pre[threadIdx.x];
+    incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;
+  }
+  __syncthreads();
+  unsigned int total = 0;
+  for (int k = 0; k < ROWS * NWP / 32; k++) total += wsum[k];
+  if (threadIdx.x < ROWS * NWP) {
+    unsigned int base = 0;
+    for (int k = 0; k < w; k++) base += wsum[k];
+    pre[threadIdx.x] = base + incl - c;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) rk[q] = pre[q * NWP + w] + __popc(bal[q] & lt);
+  __syncthreads();                       // pre and wsum may be reused
+  return total;
+}
+
+// Class of each particle: 0 its cell hosts no tracer, 1 every particle of the
+// cell takes a tracer (nt >= np), 2 contested (0 < nt < np: selection
+// sampling).  Counts the contested particles of each chunk; flags cells
+// with more than 65535 particles (the reference's uint16 counter).
+__global__ void __launch_bounds__(NT)
+class_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
+    const real *__restrict__ p2, uint32_t N, int Ng, real igs,
+    const int16_t *__restrict__ nt, const unsigned int *__restrict__ np,
+    uint8_t *__restrict__ cls, unsigned long long *cnt, int *ovf) {
+  __shared__ unsigned int pre[ROWS * NWP], wsum[ROWS * NWP / 32];
+  bool f[ROWS];
+  unsigned int rk[ROWS];
+  real pos[3];
+  const size_t b0 = (size_t) blockIdx.x * CH;
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    uint8_t k = 0;
+    if (id < N) {
+      const uint32_t c = ngp_of(p0, p1, p2, (uint32_t) id, Ng, igs, pos);
+      const int t = nt[c];
+      const unsigned int n = np[c];
+      if (n > 65535u) *ovf = 1;
+      k = (t <= 0) ? 0 : ((unsigned) t >= n ? 1 : 2);
+      cls[id] = k;
+    }
+    f[q] = k == 2;
+  }
+  const unsigned int tot = chunk_ranks(f, rk, pre, wsum);
+  if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
+}
+
+// Cell of each contested particle, in particle order.
+__global__ void __launch_bounds__(NT)
+entry_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
+    const real *__restrict__ p2, uint32_t N, int Ng, real igs,
+    const uint8_t *__restrict__ cls, const unsigned long long *__restrict__ off,
+    uint32_t *__restrict__ ecell) {
+  __shared__ unsigned int pre[ROWS * NWP], wsum[ROWS * NWP / 32];
+  bool f[ROWS];
+  unsigned int rk[ROWS];
+  real pos[3];
+  const size_t b0 = (size_t) blockIdx.x * CH;
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    f[q] = id < N && cls[id] == 2;
+  }
+  chunk_ranks(f, rk, pre, wsum);
+  const unsigned long long o = off[blockIdx.x];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++)
+    if (f[q]) {
+      const uint32_t id = (uint32_t) (b0 + (size_t) q * NT + threadIdx.x);
+      ecell[o + rk[q]] = ngp_of(p0, p1, p2, id, Ng, igs, pos);
+    }
+}
+
+// The selection-sampling chain (pop_tracer.c:838-849) over the contested
+// particles in particle order, one warp, 32 particles per step.  A particle
+// whose cell still has 0 < nt < np takes the next draw u and is kept if not
+// u np >= nt; every particle of a cell with nt > 0 decrements np, a kept one
+// nt.  When the 32 particles of a step lie in 32 different cells they are
+// decided together (each knows its draw from a ballot of the earlier ones);
+// otherwise they are decided one after another, lanes of the same cell
+// updating their copy of its counters.  Contested cells end with nt = np = 0.
+__global__ void __launch_bounds__(32)
+chain_kernel(const uint32_t *__restrict__ ecell, unsigned long long E,
+    int16_t *nt, unsigned int *np, const uint32_t *__restrict__ draws, int ran,
+    uint8_t *__restrict__ att) {
+  const int lane = threadIdx.x;
+  const unsigned int full = 0xffffffffu, lt = (1u << lane) - 1;
+  unsigned long long d = 0;
+  for (unsigned long long b = 0; b < E; b += 32) {
+    const unsigned long long e = b + lane;
+    const bool valid = e < E;
+    const uint32_t c = valid ? ecell[e] : 0xffffffffu;
+    int tn = valid ? nt[c] : 0;
+    int pn = valid ? (int) np[c] : 0;
+    const uint32_t u = (d + lane < E) ? draws[d + lane] : 0u;
+    const unsigned int same = __match_any_sync(full, c);
+    const bool dup = __any_sync(full, valid && __popc(same) > 1);
+    bool kept = false;
+    int used;
+    if (!dup) {
+      const bool cons = valid && tn > 0 && tn < pn;
+      const unsigned int cm = __ballot_sync(full, cons);
+      const uint32_t uk = __shfl_sync(full, u, __popc(cm & lt));
+      if (valid && tn > 0) {
+        kept = !cons || !(ez_u(ran, uk) * pn >= tn);
+        pn -= 1;
+        tn -= kept ? 1 : 0;
+      }
+      used = __popc(cm);
+    }
+    else {
+      used = 0;
+      for (int i = 0; i < 32; i++) {
+        const uint32_t ci = __shfl_sync(full, c, i);
+        const int ti = __shfl_sync(full, tn, i), pi = __shfl_sync(full, pn, i);
+        const int vi = __shfl_sync(full, (int) valid, i);
+        const uint32_t ui = __shfl_sync(full, u, used);
+        bool ki = false, cons = false;
+        if (vi && ti > 0) {
+          cons = ti < pi;
+          ki = !cons || !(ez_u(ran, ui) * pi >= ti);
+        }
+        if (lane == i) kept = ki;
+        if (vi && ti > 0 && valid && c == ci) {
+          pn = pi - 1;
+          tn = ti - (ki ? 1 : 0);
+        }
+        used += cons ? 1 : 0;
+      }
+    }
+    if (valid) {
+      nt[c] = (int16_t) tn;
+      np[c] = (unsigned int) pn;
+      att[e] = kept ? 1 : 0;
+    }
+    __syncwarp();
+    d += (unsigned long long) used;
+  }
+}
+
+// Attached particles of each chunk (class 1, or class 2 and kept).
+__global__ void __launch_bounds__(NT)
+att_count_kernel(uint32_t N, const uint8_t *__restrict__ cls,
+    const unsigned long long *__restrict__ eoff, const uint8_t *__restrict__ att,
+    unsigned long long *cnt) {
+  __shared__ unsigned int pre[ROWS * NWP], wsum[ROWS * NWP / 32];
+  bool f[ROWS];
+  unsigned int rk[ROWS];
+  uint8_t k[ROWS];
+  const size_t b0 = (size_t) blockIdx.x * CH;
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    k[q] = (id < N) ? cls[id] : 0;
+    f[q] = k[q] == 2;
+  }
+  chunk_ranks(f, rk, pre, wsum);
+  const unsigned long long o = eoff[blockIdx.x];
+  unsigned int n = 0;
+#pragma unroll
+  for (int q = 0; q < ROWS; q++)
+    n += (k[q] == 1 || (k[q] == 2 && att[o + rk[q]])) ? 1 : 0;
+#pragma unroll
+  for (int m = 16; m; m >>= 1) n += __shfl_xor_sync(0xffffffffu, n, m);
+  if (threadIdx.x == 0) pre[0] = 0;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) atomicAdd(&pre[0], n);
+  __syncthreads();
+  if (threadIdx.x == 0) cnt[blockIdx.x] = pre[0];
+}
+
+// Attached tracers in particle order: position = particle position, velocity
+// = psi vfac (pop_tracer.c:855-871).
+__global__ void __launch_bounds__(NT)
+att_write_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
+    const real *__restrict__ p2, uint32_t N, int Ng, real igs, real gs,
+    double vfac, const uint8_t *__restrict__ cls,
+    const unsigned long long *__restrict__ eoff, const uint8_t *__restrict__ att,
+    const unsigned long long *__restrict__ aoff, real *x, real *y, real *z,
+    real *vx, real *vy, real *vz) {
+  __shared__ unsigned int pre[ROWS * NWP], wsum[ROWS * NWP / 32];
+  bool f[ROWS], a[ROWS];
+  unsigned int rk[ROWS], ra[ROWS];
+  uint8_t k[ROWS];
+  const size_t b0 = (size_t) blockIdx.x * CH;
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
+    k[q] = (id < N) ? cls[id] : 0;
+    f[q] = k[q] == 2;
+  }
+  chunk_ranks(f, rk, pre, wsum);
+  const unsigned long long oe = eoff[blockIdx.x];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) a[q] = k[q] == 1 || (k[q] == 2 && att[oe + rk[q]]);
+  chunk_ranks(a, ra, pre, wsum);
+  const unsigned long long oa = aoff[blockIdx.x];
+  real pos[3];
+#pragma unroll
+  for (int q = 0; q < ROWS; q++)
+    if (a[q]) {
+      const uint32_t id = (uint32_t) (b0 + (size_t) q * NT + threadIdx.x);
+      ngp_of(p0, p1, p2, id, Ng, igs, pos);
+      const unsigned long long t = oa + ra[q];
+      x[t] = pos[0] * gs;
+      y[t] = pos[1] * gs;
+      z[t] = pos[2] * gs;
+      vx[t] = p0[id] * vfac;
+      vy[t] = p1[id] * vfac;
+      vz[t] = p2[id] * vfac;
+    }
+}
+
+// Tracers left per cell once the particles are taken: nt - np where every
+// particle was attached; contested cells are already at nt = 0.
+__global__ void __launch_bounds__(NT)
+leftover_kernel(int16_t *nt, const unsigned int *__restrict__ np, uint32_t N) {
+  for (uint32_t c = blockIdx.x * NT + threadIdx.x; c < N; c += gridDim.x * NT) {
+    const int t = nt[c];
+    if (t > 0) nt[c] = (int16_t) max(t - (int) np[c], 0);
   }
 }
 
@@ -623,6 +914,21 @@ disp_kernel(size_t n, const uint32_t *__restrict__ draws, int ran,
 unsigned grid_for(size_t n, int nt) {
   const size_t b = (n + nt - 1) / nt;
   return (unsigned) (b < 148 * 32 ? (b ? b : 1) : 148 * 32);
+}
+
+// Buffer of the attach-to-particle stage, grown on demand.
+int att_buffer(EzMesh *m, size_t bytes) {
+  if (bytes <= m->att_cap) return 0;
+  if (m->att) {
+    cudaStreamSynchronize(m->stream);
+    cudaFree(m->att);
+  }
+  m->att = nullptr;
+  m->att_cap = 0;
+  bytes = (bytes + 4095) / 4096 * 4096;
+  if (!EZ_CUDA_OK(cudaMalloc(&m->att, bytes))) { cudaGetLastError(); return EZMOCK_ERR_MEMORY; }
+  m->att_cap = bytes;
+  return 0;
 }
 
 int ensure_draws(EzMesh *m, size_t count) {
@@ -772,7 +1078,7 @@ int ez_select_counts(EzMesh *m, const unsigned long long *h, size_t *pdf,
 
 int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
     double vfac, const real *params, const size_t *pdf, int nmax,
-    size_t ncell, size_t ntot, EzPopResult *res) {
+    size_t ncell, size_t ntot, bool att_part, EzPopResult *res) {
   const size_t N = m->N;
   const real rho_c = params[0], rho_exp = params[1], sigma_v = params[3];
   const real thres = (rho_c == 0) ? (real) EZ_REAL_MIN : rho_c;
@@ -850,42 +1156,108 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   m->cat_n = nt_all;
   real *cx = m->cat, *cy = cx + nt_all, *cz = cy + nt_all;
   real *cvx = cz + nt_all, *cvy = cvx + nt_all, *cvz = cvy + nt_all;
-  tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt); ez_count_launch();
+  const real gs = Lbox / Ng;
+  const real igs = Ng / Lbox;
+
+  // tracers attached to particles first (att_part)
+  size_t iv = 0;
+  int16_t *nt16 = nullptr;
+  if (att_part) {
+    if (N > 0xffffffffULL) return EZMOCK_ERR_UNKNOWN;
+    nt16 = (int16_t *) m->spec[2];
+    unsigned int *np32 = (unsigned int *) m->spec[1];
+    uint8_t *cls = (uint8_t *) m->spec[0];       // after rho_t is read below
+    const uint32_t N32 = (uint32_t) N;
+    nt_kernel<<<grid_for(N, NT), NT, 0, st>>>(rhot, N, bo, nt16); ez_count_launch();
+    if (!EZ_CUDA_OK(cudaMemsetAsync(np32, 0, N * sizeof(unsigned int), st)))
+      return EZMOCK_ERR_UNKNOWN;
+    np_kernel<<<grid_for(N, NT), NT, 0, st>>>(m->psi[0], m->psi[1], m->psi[2], N32, Ng,
+        igs, nt16, np32); ez_count_launch();
+    // chunk offsets of the attached particles and an overflow flag
+    const size_t aoff_b = (nblk + 1) * sizeof(unsigned long long);
+    if ((e = att_buffer(m, 2 * aoff_b + 256))) return e;
+    unsigned long long *acnt = (unsigned long long *) m->att;
+    unsigned long long *aoff = acnt + (nblk + 1);
+    int *ovf = (int *) (aoff + (nblk + 1));
+    if (!EZ_CUDA_OK(cudaMemsetAsync(ovf, 0, sizeof(int), st))) return EZMOCK_ERR_UNKNOWN;
+    class_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->psi[0], m->psi[1], m->psi[2], N32, Ng,
+        igs, nt16, np32, cls, bcnt, ovf); ez_count_launch();
+    scan_u64(bcnt, bscan, nblk, ps.tmp, st);
+    unsigned long long E = 0;
+    int hovf = 0;
+    if (!EZ_CUDA_OK(cudaMemcpyAsync(&E, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
+        !EZ_CUDA_OK(cudaMemcpyAsync(&hovf, ovf, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+      return EZMOCK_ERR_UNKNOWN;
+    if (hovf) { res->err = EZMOCK_ERR_RHO_NPART; return 0; }
+    // contested particles: their cells, the draws of the chain (from 4N), the
+    // kept flags
+    if ((e = att_buffer(m, 2 * aoff_b + 256 + E * (sizeof(uint32_t) + 1)))) return e;
+    acnt = (unsigned long long *) m->att;
+    aoff = acnt + (nblk + 1);
+    uint32_t *ecell = (uint32_t *) ((char *) m->att + 2 * aoff_b + 256);
+    uint8_t *kept = (uint8_t *) (ecell + E);
+    if (E) {
+      entry_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->psi[0], m->psi[1], m->psi[2], N32, Ng,
+          igs, cls, bscan, ecell); ez_count_launch();
+      if ((e = ensure_draws(m, E))) return e;
+      if ((e = ez_rng_fill_free(m, ran, seed, (uint64_t) N << 2, E, m->draws))) return e;
+      chain_kernel<<<1, 32, 0, st>>>(ecell, E, nt16, np32, m->draws, ran, kept);
+      ez_count_launch();
+    }
+    att_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(N32, cls, bscan, kept, acnt); ez_count_launch();
+    scan_u64(acnt, aoff, nblk, ps.tmp, st);
+    unsigned long long na = 0;
+    if (!EZ_CUDA_OK(cudaMemcpyAsync(&na, aoff + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
+        !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+      return EZMOCK_ERR_UNKNOWN;
+    if (na > nt_all) { res->err = EZMOCK_ERR_UNKNOWN; return 0; }
+    iv = (size_t) na;
+    if (iv) {
+      att_write_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->psi[0], m->psi[1], m->psi[2], N32,
+          Ng, igs, gs, vfac, cls, bscan, kept, aoff, cx, cy, cz, cvx, cvy, cvz);
+      ez_count_launch();
+    }
+    leftover_kernel<<<grid_for(N, NT), NT, 0, st>>>(nt16, np32, N32); ez_count_launch();
+  }
+  const size_t nrand = nt_all - iv;              // tracers at random cell positions
+
+  tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt, nt16); ez_count_launch();
   scan_u64(bcnt, bscan, nblk, ps.tmp, st);
   unsigned long long ncount = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(&ncount, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
     return EZMOCK_ERR_UNKNOWN;
   // the per-cell counts must add up to the selected total (pop_tracer.c:989-993)
-  if (ncount != nt_all) { res->err = EZMOCK_ERR_UNKNOWN; return 0; }
-  if ((e = ensure_draws(m, std::max((size_t) 3 * nt_all, (size_t) 1)))) return e;
+  if (ncount != nrand) { res->err = EZMOCK_ERR_UNKNOWN; return 0; }
+  if ((e = ensure_draws(m, std::max((size_t) 3 * nrand, (size_t) 1)))) return e;
   const uint32_t *dpos = nullptr;
-  if ((e = ez_rng_draws(m, ran, seed, 1, 3 * nt_all, m->draws, &dpos))) return e;
-  const real gs = Lbox / Ng;
+  if ((e = ez_rng_draws(m, ran, seed, 1, 3 * nrand, m->draws, &dpos))) return e;
   // tracer cell indices in the velocity arrays (written later)
   if (N <= 0xffffffffULL) {
-    uint32_t *cid = (uint32_t *) cvx;
+    uint32_t *cid = (uint32_t *) (cvx + iv);
     tracer_cell_kernel<uint32_t><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
-        (unsigned long long) nt_all, cid); ez_count_launch();
-    if (nt_all)
-      place_kernel<uint32_t><<<grid_for(nt_all, NT), NT, 0, st>>>(cid, nt_all, Ng,
-          dpos, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
+        (unsigned long long) nrand, cid, nt16); ez_count_launch();
+    if (nrand)
+      place_kernel<uint32_t><<<grid_for(nrand, NT), NT, 0, st>>>(cid, nrand, Ng,
+          dpos, ran, gs, Lbox, cx + iv, cy + iv, cz + iv); ez_count_launch();
   }
   else {
-    unsigned long long *cid = (unsigned long long *) cvx;      // vx and vy
+    unsigned long long *cid = (unsigned long long *) cvx;      // vx and vy (iv = 0)
     tracer_cell_kernel<unsigned long long><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo,
-        bscan, (unsigned long long) nt_all, cid); ez_count_launch();
-    if (nt_all)
-      place_kernel<unsigned long long><<<grid_for(nt_all, NT), NT, 0, st>>>(cid, nt_all,
+        bscan, (unsigned long long) nrand, cid, nt16); ez_count_launch();
+    if (nrand)
+      place_kernel<unsigned long long><<<grid_for(nrand, NT), NT, 0, st>>>(cid, nrand,
           Ng, dpos, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
   }
   ez_stage_end(m, ST_EMIT);
 
   // ---- 5./6. velocities and dispersion ----
   ez_stage_begin(m, ST_VEL);
-  const real igs = Ng / Lbox;
-  vel_kernel<<<grid_for(nt_all, NT), NT, 0, st>>>(m->rho, m->paint[0],
-      m->paint[1], m->paint[2], Ng, igs, vfac, nt_all, cx, cy, cz, cvx, cvy, cvz); ez_count_launch();
+  if (nrand)
+    vel_kernel<<<grid_for(nrand, NT), NT, 0, st>>>(m->rho, m->paint[0],
+        m->paint[1], m->paint[2], Ng, igs, vfac, nrand, cx + iv, cy + iv, cz + iv, cvx + iv,
+        cvy + iv, cvz + iv); ez_count_launch();
   const size_t nd_disp = 6 * ((nt_all + 1) / 2);
   if ((e = ensure_draws(m, std::max(nd_disp, (size_t) 1)))) return e;
   const uint32_t *ddisp = nullptr;

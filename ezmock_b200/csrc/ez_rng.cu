@@ -853,6 +853,13 @@ int ez_rng_fill_around(EzMesh *m, int ran, uint64_t seed, uint64_t start,
   return e;
 }
 
+int ez_rng_fill_free(EzMesh *m, int ran, uint64_t seed, uint64_t start,
+    uint64_t count, uint32_t *out) {
+  if (ran == EZMOCK_RNG_MT19937)
+    return mt_fill(m, seed, start, count, out, m->rng_nprep ? m->rng_prep_end : 0);
+  return mrg_fill(m, seed, start, count, out);
+}
+
 int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
     uint64_t count, uint32_t *out) {
   m->rng_nprep = 0;                         // the scratch is reused
