@@ -685,20 +685,32 @@ entry_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
 // decided together (each knows its draw from a ballot of the earlier ones);
 // otherwise they are decided one after another, lanes of the same cell
 // updating their copy of its counters.  Contested cells end with nt = np = 0.
+// The next step's cells, counters and 64 draws (it starts within 32 draws of
+// the current one) are loaded before the current step is decided; counters
+// of cells the current step changes are then taken from its lanes.
 __global__ void __launch_bounds__(32)
 chain_kernel(const uint32_t *__restrict__ ecell, unsigned long long E,
     int16_t *nt, unsigned int *np, const uint32_t *__restrict__ draws, int ran,
     uint8_t *__restrict__ att) {
   const int lane = threadIdx.x;
   const unsigned int full = 0xffffffffu, lt = (1u << lane) - 1;
-  unsigned long long d = 0;
+  unsigned long long d = 0;                  // draws used before this step
+  // step 0
+  bool valid = (unsigned long long) lane < E;
+  uint32_t c = valid ? ecell[lane] : 0xffffffffu;
+  int tn = valid ? nt[c] : 0;
+  int pn = valid ? (int) np[c] : 0;
+  uint32_t w0 = ((unsigned long long) lane < E) ? draws[lane] : 0u;
+  uint32_t w1 = (32ull + lane < E) ? draws[32 + lane] : 0u;
   for (unsigned long long b = 0; b < E; b += 32) {
-    const unsigned long long e = b + lane;
-    const bool valid = e < E;
-    const uint32_t c = valid ? ecell[e] : 0xffffffffu;
-    int tn = valid ? nt[c] : 0;
-    int pn = valid ? (int) np[c] : 0;
-    const uint32_t u = (d + lane < E) ? draws[d + lane] : 0u;
+    // prefetch of the next step
+    const unsigned long long e1 = b + 32 + lane;
+    const bool valid1 = e1 < E;
+    const uint32_t c1 = valid1 ? ecell[e1] : 0xffffffffu;
+    int tn1 = valid1 ? nt[c1] : 0;
+    int pn1 = valid1 ? (int) np[c1] : 0;
+    const uint32_t nx = (d + 64 + lane < E) ? draws[d + 64 + lane] : 0u;   // draw d+64+lane
+    // this step; its draws are w0 (d .. d+31)
     const unsigned int same = __match_any_sync(full, c);
     const bool dup = __any_sync(full, valid && __popc(same) > 1);
     bool kept = false;
@@ -706,7 +718,7 @@ chain_kernel(const uint32_t *__restrict__ ecell, unsigned long long E,
     if (!dup) {
       const bool cons = valid && tn > 0 && tn < pn;
       const unsigned int cm = __ballot_sync(full, cons);
-      const uint32_t uk = __shfl_sync(full, u, __popc(cm & lt));
+      const uint32_t uk = __shfl_sync(full, w0, __popc(cm & lt));
       if (valid && tn > 0) {
         kept = !cons || !(ez_u(ran, uk) * pn >= tn);
         pn -= 1;
@@ -720,7 +732,7 @@ chain_kernel(const uint32_t *__restrict__ ecell, unsigned long long E,
         const uint32_t ci = __shfl_sync(full, c, i);
         const int ti = __shfl_sync(full, tn, i), pi = __shfl_sync(full, pn, i);
         const int vi = __shfl_sync(full, (int) valid, i);
-        const uint32_t ui = __shfl_sync(full, u, used);
+        const uint32_t ui = __shfl_sync(full, w0, used);
         bool ki = false, cons = false;
         if (vi && ti > 0) {
           cons = ti < pi;
@@ -737,10 +749,25 @@ chain_kernel(const uint32_t *__restrict__ ecell, unsigned long long E,
     if (valid) {
       nt[c] = (int16_t) tn;
       np[c] = (unsigned int) pn;
-      att[e] = kept ? 1 : 0;
+      att[b + lane] = kept ? 1 : 0;
+    }
+    // counters of the next step that this step changed
+    for (int i = 0; i < 32; i++) {
+      const uint32_t ci = __shfl_sync(full, c, i);
+      const int ti = __shfl_sync(full, tn, i), pi = __shfl_sync(full, pn, i);
+      const int vi = __shfl_sync(full, (int) valid, i);
+      if (vi && valid1 && c1 == ci) { tn1 = ti; pn1 = pi; }
     }
     __syncwarp();
+    // window of the next step, draws d + used + (0 .. 63), out of the draws
+    // d .. d+95 held in w0 | w1 | nx (used <= 32)
+    const int s0 = lane + used, src = s0 & 31;
+    const uint32_t a0 = __shfl_sync(full, w0, src), a1 = __shfl_sync(full, w1, src),
+                   a2 = __shfl_sync(full, nx, src);
+    w0 = (s0 < 32) ? a0 : a1;                 // draw d + s0
+    w1 = (s0 < 32) ? a1 : a2;                 // draw d + 32 + s0
     d += (unsigned long long) used;
+    c = c1; tn = tn1; pn = pn1; valid = valid1;
   }
 }
 
