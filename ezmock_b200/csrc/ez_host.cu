@@ -12,6 +12,9 @@
 #include <atomic>
 #include <cmath>
 #include <thread>
+
+#include <omp.h>
+#include <sys/mman.h>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -602,6 +605,23 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
       return (*err = EZMOCK_ERR_MEMORY);
     }
   }
+  int nthr = CONF(ez)->nthread > 0 ? CONF(ez)->nthread : omp_get_num_procs();
+  nthr = std::max(1, std::min(nthr, 8));
+  // The arrays are fresh malloc() memory: ask for huge pages and fault them
+  // in with several threads while the GPU finishes the catalogue, so the
+  // copy-out below runs at memcpy speed.
+  const size_t bytes_arr = n * sizeof(real);
+  if (bytes_arr >= ((size_t) 4 << 20)) {
+    const size_t pg = 4096, npg = (bytes_arr + pg - 1) / pg;
+    for (int a = 0; a < 6; a++) {
+      const uintptr_t b = ((uintptr_t) cat[a] + pg - 1) & ~(uintptr_t) (pg - 1);
+      const uintptr_t e = ((uintptr_t) cat[a] + bytes_arr) & ~(uintptr_t) (pg - 1);
+      if (e > b) madvise((void *) b, e - b, MADV_HUGEPAGE);
+    }
+#pragma omp parallel for num_threads(nthr) schedule(static)
+    for (long p = 0; p < (long) (6 * npg); p++)
+      ((volatile char *) cat[p / npg])[(p % npg) * pg] = 0;
+  }
   // device -> pinned staging (two 8 MB halves, DMA of one overlapping the
   // copy-out of the other) -> the caller's malloc() arrays, copied out by
   // several host threads
@@ -621,9 +641,6 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
     cudaEventCreateWithFlags(&m->d2h_ev[0], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&m->d2h_ev[1], cudaEventDisableTiming);
   }
-  int nthr = CONF(ez)->nthread > 0 ? CONF(ez)->nthread : (int) std::thread::hardware_concurrency();
-  nthr = std::max(1, std::min(nthr, 8));
-  const size_t bytes_arr = n * sizeof(real);
   const size_t per = half / sizeof(real);               // reals per half
   struct Piece { int arr; size_t off, len; };
   std::vector<Piece> pieces;
@@ -651,16 +668,14 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
     const int nt = (nb >= ((size_t) 1 << 20)) ? nthr : 1;
     if (nt == 1) memcpy(dst, src, nb);
     else {
-      std::vector<std::thread> th;
       const size_t step = (nb + nt - 1) / nt;
+#pragma omp parallel for num_threads(nt) schedule(static)
       for (int t = 0; t < nt; t++) {
         const size_t b0 = std::min(nb, t * step), b1 = std::min(nb, b0 + step);
-        if (b1 > b0) th.emplace_back([=]() { memcpy(dst + b0, src + b0, b1 - b0); });
+        if (b1 > b0) memcpy(dst + b0, src + b0, b1 - b0);
       }
-      for (auto &x : th) x.join();
     }
   }
-  (void) bytes_arr;
   if (!ok) {
     for (int j = 0; j < 6; j++) free(cat[j]);
     return (*err = EZMOCK_ERR_UNKNOWN);
