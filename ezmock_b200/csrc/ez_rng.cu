@@ -355,7 +355,7 @@ constexpr int R_THREADS = 256;
 __global__ void __launch_bounds__(R_THREADS)
 mt_ring_kernel(const uint32_t *__restrict__ states, uint64_t L, uint64_t count,
     uint32_t *__restrict__ out) {
-  __shared__ uint32_t ring[1024];
+  __shared__ uint32_t ring[2048];
   const int t = threadIdx.x;
   const uint64_t c0 = (uint64_t) blockIdx.x * L;
   if (c0 >= count) return;
@@ -363,12 +363,22 @@ mt_ring_kernel(const uint32_t *__restrict__ states, uint64_t L, uint64_t count,
   for (int k = t; k < MT_N; k += R_THREADS) ring[k] = states[(size_t) blockIdx.x * MT_N + k];
   __syncthreads();
   uint32_t *o = out + c0;
-  for (uint64_t g = 0; g < n; g += MT_N - MT_M) {
-    if (t < MT_N - MT_M && g + t < n) {
-      const uint32_t b = (uint32_t) g + t;   // logical index mod 2^32; 1024 | 2^32
-      const uint32_t y = mt_f(ring[b & 1023], ring[(b + 1) & 1023], ring[(b + MT_M) & 1023]);
-      ring[(b + MT_N) & 1023] = y;
-      o[g + t] = mt_temper(y);
+  // Two steps of S = 227 words between barriers.  Step two's third operand
+  // x[b + S + 397] = x[b + 624] is step one's result in the same thread.
+  // A group reads ring words [g, g + 624) and writes [g + 624, g + 1078);
+  // both spans together are shorter than the ring, and the words it
+  // overwrites, [g - 1424, g - 970) mod 2048, are no longer needed.
+  constexpr int S = MT_N - MT_M;
+  for (uint64_t g = 0; g < n; g += 2 * S) {
+    if (t < S) {
+      const uint32_t b = (uint32_t) g + t;   // logical index mod 2^32; 2048 | 2^32
+      const uint32_t y = mt_f(ring[b & 2047], ring[(b + 1) & 2047], ring[(b + MT_M) & 2047]);
+      ring[(b + MT_N) & 2047] = y;
+      if (g + t < n) o[g + t] = mt_temper(y);
+      const uint32_t b2 = b + S;
+      const uint32_t y2 = mt_f(ring[b2 & 2047], ring[(b2 + 1) & 2047], y);
+      ring[(b2 + MT_N) & 2047] = y2;
+      if (g + S + t < n) o[g + S + t] = mt_temper(y2);
     }
     __syncthreads();
   }
