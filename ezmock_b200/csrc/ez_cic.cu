@@ -91,22 +91,24 @@ cic_atomic_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
 // ---- owner-computes kernel (FP32) ----
 //
 // A CTA owns a 16 x 16 column of output cells (all z) and walks it along z in
-// chunks of 8 slices.  For each chunk it reads every particle whose
-// Lagrangian cell lies within OH = 3 cells of the column (23 x 23 x 8
-// particles) and keeps the CIC contributions that land in its own cells, in a
-// shared-memory ring of three z chunks.  Accumulation is in 32-bit fixed
-// point (integer shared-memory atomics are exact and fast): rho in units of
-// 2^-21 per cell, the momenta in units of 2^-s with s chosen from the largest
-// |psi| so that no sum can overflow while rho < 1024.  A chunk is final once
-// the particles of the next chunk are in; it is then written with plain
-// coalesced stores, so every output cell is written exactly once and no
-// global atomics are needed.  Particles displaced by more than OH cells in
+// chunks of 8 slices.  For each chunk it reads every particle whose cloud can
+// reach the column -- Lagrangian cells i0 - OH - 1 .. i0 + 15 + OH in x (the
+// lower corner moves by at most OH cells, the upper corner lies one cell
+// above it) and likewise in y, (17 + 2 OH)^2 x 8 particles -- and keeps the
+// CIC contributions that land in its own cells, in a shared-memory ring of
+// three z chunks.  OH is 2 or 3: an instance starts with 2 and moves to 3
+// when more than 1/64 of the particles lie farther than 2 cells from their
+// Lagrangian cell (every launch counts them).  Accumulation is in 32-bit
+// fixed point (integer shared-memory atomics are exact and fast): rho in
+// units of 2^-21 per cell, the momenta in units of 2^-s with s chosen from
+// the largest |psi| so that no sum can overflow while rho < 1024.  A chunk is
+// final once the particles of the next chunk are in; it is then written with
+// plain coalesced stores, so every output cell is written exactly once and
+// no global atomics are needed.  Particles displaced by more than OH cells in
 // any direction are listed by their own CTA and deposited afterwards with
 // global atomics (fixup_kernel).  A negative rho sum (overflow) raises a flag
 // on which the host repeats the assignment with float atomics.
 constexpr int OT = 16;                       // owned column tile (x and y)
-constexpr int OH = 3;                        // halo: largest in-kernel |offset|
-constexpr int OW = OT + 2 * OH + 1;          // particle read width = 23
 constexpr int OKZ = 8;                       // z slices per chunk
 constexpr int ORS = 3 * OKZ;                 // ring: three chunks
 constexpr int OWN_NT = 512;
@@ -137,8 +139,10 @@ __device__ __forceinline__ int wrap1(int v, int Ng) {
 // mantissa bits, rounded to nearest even (the default rounding of the add),
 // so the result equals __float2int_rn(v).
 constexpr float RMAGIC = 12582912.f;         // 1.5 * 2^23
-__device__ __forceinline__ int fround(float v) {
-  return __float_as_int(v + RMAGIC) - 0x4B400000;
+// round(a * b) of the exact product, |a * b| < 2^22: the magic addition is
+// fused into the multiply (one rounding).
+__device__ __forceinline__ int fmround(float a, float b) {
+  return __float_as_int(__fmaf_rn(a, b, RMAGIC)) - 0x4B400000;
 }
 // floor(v) for |v| < 2^22, exact: round, then step down where rounding went up.
 __device__ __forceinline__ int ffloor(float v) {
@@ -147,10 +151,13 @@ __device__ __forceinline__ int ffloor(float v) {
   return __float_as_int(t) - 0x4B400000 - (r > v ? 1 : 0);
 }
 
+template <int OH>
 __global__ void __launch_bounds__(OWN_NT, 2)
 cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
     const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
     int Ng, real igs, CicStats *stats, unsigned int *list) {
+  constexpr int OW = OT + 2 * OH + 1;        // particle read width
+  constexpr int OB = OH + 1;                 // read origin: i0 - OB, j0 - OB
   extern __shared__ __align__(16) int iring[];       // [4][OT*OT][ORS]
   const int nt = Ng / OT;
   const int i0 = (blockIdx.x / nt) * OT, j0 = (blockIdx.x % nt) * OT;
@@ -172,8 +179,8 @@ cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
       const int kz = p & (OKZ - 1), lc = p >> 3;
       li = lc / OW;
       lj = lc - li * OW;
-      iw = wrap1(i0 - OH + li, Ng);
-      jw = wrap1(j0 - OH + lj, Ng);
+      iw = wrap1(i0 - OB + li, Ng);
+      jw = wrap1(j0 - OB + lj, Ng);
       zu = c * OKZ + kz;
       zw = wrap1(zu, Ng);
       return ((size_t) iw * Ng + jw) * Ng + zw;
@@ -199,20 +206,29 @@ cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
       const int x0 = ffloor(x), y0 = ffloor(y), z0 = ffloor(z);
       const int dx = x0 - iw, dy = y0 - jw, dz = z0 - zw;
       const bool far = dx < -OH || dx > OH || dy < -OH || dy > OH || dz < -OH || dz > OH;
-      const bool own = cown && li >= OH && li < OH + OT && lj >= OH && lj < OH + OT;
+      const bool own = cown && li >= OB && li < OB + OT && lj >= OB && lj < OB + OT;
       const unsigned am = __activemask();
+      if (OH > 2) {
+        // particles that a launch with OH = 2 would list
+        const bool far2 = dx < -2 || dx > 2 || dy < -2 || dy > 2 || dz < -2 || dz > 2;
+        const unsigned f2 = __ballot_sync(am, far2 && own);
+        if (f2 && lane == __ffs(f2) - 1) atomicAdd(&stats->nfar2, (unsigned) __popc(f2));
+      }
       const unsigned fm = __ballot_sync(am, far && own);
       if (fm) {
         const int leader = __ffs(fm) - 1;
         unsigned int base = 0;
-        if (lane == leader) base = atomicAdd(&stats->nlist, (unsigned) __popc(fm));
+        if (lane == leader) {
+          base = atomicAdd(&stats->nlist, (unsigned) __popc(fm));
+          if (OH == 2) atomicAdd(&stats->nfar2, (unsigned) __popc(fm));
+        }
         base = __shfl_sync(am, base, leader);
         if (far && own) list[base + __popc(fm & ((1u << lane) - 1))] = (unsigned int) id;
       }
       if (far) continue;
       // tile coordinates of the lower corner; skip particles whose cloud
       // misses the tile
-      const int cx = li - OH + dx, cy = lj - OH + dy, zz = zu + dz;
+      const int cx = li - OB + dx, cy = lj - OB + dy, zz = zu + dz;
       const bool ax0 = (unsigned) cx < (unsigned) OT, ax1 = (unsigned) (cx + 1) < (unsigned) OT;
       const bool by0 = (unsigned) cy < (unsigned) OT, by1 = (unsigned) (cy + 1) < (unsigned) OT;
       const bool cz0 = (unsigned) zz < (unsigned) Ng, cz1 = (unsigned) (zz + 1) < (unsigned) Ng;
@@ -245,10 +261,10 @@ cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
         for (int ic = 0; ic < 2; ic++) {
           if (!okz[ic]) continue;
           int *r = iring + oxy + ss[ic];
-          atomicAdd(r, fround(w * zr[ic]));
-          atomicAdd(r + OQS, fround(w * za[ic]));
-          atomicAdd(r + 2 * OQS, fround(w * zb[ic]));
-          atomicAdd(r + 3 * OQS, fround(w * zc[ic]));
+          atomicAdd(r, fmround(w, zr[ic]));
+          atomicAdd(r + OQS, fmround(w, za[ic]));
+          atomicAdd(r + 2 * OQS, fmround(w, zb[ic]));
+          atomicAdd(r + 3 * OQS, fmround(w, zc[ic]));
         }
       }
     }
@@ -395,7 +411,8 @@ int ez_cic(EzMesh *m, double Lbox) {
       static bool attr = false;
       const size_t smem = 4 * OQS * sizeof(int);
       if (!attr) {
-        cudaFuncSetAttribute(cic_owner_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaFuncSetAttribute(cic_owner_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaFuncSetAttribute(cic_owner_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
         attr = true;
       }
       CicStats *stats = (CicStats *) m->stats;
@@ -404,18 +421,26 @@ int ez_cic(EzMesh *m, double Lbox) {
         cudaMemsetAsync(&stats->psimax_bits, 0, sizeof(unsigned int), m->stream);
         psi_absmax_kernel<<<148 * 8, 256, 0, m->stream>>>(m->psi[0], 3 * N, stats); ez_count_launch();
       }
-      cudaMemsetAsync(&stats->nlist, 0, 2 * sizeof(int), m->stream);
-      cic_owner_kernel<<<(unsigned) ((Ng / OT) * (Ng / OT)), OWN_NT, smem, m->stream>>>(
-          m->psi[0], m->psi[1], m->psi[2], m->rho, m->paint[0], m->paint[1],
-          m->paint[2], Ng, igs, stats, list); ez_count_launch();
+      cudaMemsetAsync(&stats->nlist, 0, 3 * sizeof(int), m->stream);
+      const unsigned nblk = (unsigned) ((Ng / OT) * (Ng / OT));
+      if (m->cic_oh == 3)
+        cic_owner_kernel<3><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
+            m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
+      else
+        cic_owner_kernel<2><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
+            m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
+      ez_count_launch();
       fixup_kernel<<<148 * 4, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
           m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs,
           stats, list); ez_count_launch();
-      int ovf = 0;
-      if (!EZ_CUDA_OK(cudaMemcpyAsync(&ovf, &stats->overflow, sizeof(int), cudaMemcpyDeviceToHost, m->stream)) ||
+      int res[2] = {0, 0};                            // overflow, nfar2
+      if (!EZ_CUDA_OK(cudaMemcpyAsync(res, &stats->overflow, sizeof(res), cudaMemcpyDeviceToHost, m->stream)) ||
           !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
         return EZMOCK_ERR_UNKNOWN;
-      if (ovf) {
+      // the halo for the next field of this instance: 2 while few particles
+      // move farther (they go through the global-atomic fixup)
+      m->cic_oh = ((size_t) (unsigned) res[1] > N / 64) ? 3 : 2;
+      if (res[0]) {
         // a cell holds >= 1024 particles: repeat with float atomics
         cudaMemsetAsync(m->rho, 0, N * sizeof(real), m->stream);
         for (int d = 0; d < 3; d++) cudaMemsetAsync(m->paint[d], 0, N * sizeof(real), m->stream);

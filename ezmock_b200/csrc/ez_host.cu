@@ -859,6 +859,10 @@ int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
       if (value <= 0) return (*err = EZMOCK_ERR_ARG_SEED);
       RNG(ez)->seed = (uint64_t) value;
       return 0;
+    case EZMOCKB200_OPT_CIC_HALO:
+      if (value != 2 && value != 3) return (*err = EZMOCK_ERR_ARG_PARAMS);
+      m->cic_oh = (int) value;
+      return 0;
     default: return (*err = EZMOCK_ERR_ARG_PARAMS);
   }
 }

@@ -83,6 +83,7 @@ struct EzMesh {
   int timing;              // record per-stage events
   cudaEvent_t mark[8];     // caller-placed events on the instance stream
   int cic_mode;            // 0: float atomics, 1: deterministic fixed-point
+  int cic_oh;              // halo of the owner-computes CIC (3; otherwise 2)
 
   int Ng;
   size_t N;                // Ng^3
@@ -137,7 +138,7 @@ struct EzCicStats {
   unsigned int psimax_bits;   // max |psi| over the three fields (float bits)
   unsigned int nlist;         // far-displaced particles listed for fixup
   int overflow;               // a fixed-point cell sum overflowed
-  int pad;
+  unsigned int nfar2;         // particles displaced by more than 2 cells on some axis
 };
 
 // ---- error helpers ----

@@ -20,6 +20,11 @@ extern "C" {
 #define EZMOCKB200_OPT_TIMING   2   /* 1: record per-stage CUDA-event timings */
 #define EZMOCKB200_OPT_DEVICE   3   /* CUDA device ordinal (before the first field) */
 #define EZMOCKB200_OPT_SEED     4   /* new random seed (> 0) for the next field */
+/* Halo (2 or 3 cells) of the FP32 density assignment for the next field.
+   Particles displaced farther go through a slower global-atomic pass; after
+   each field the engine picks 3 when more than 1/64 of the particles moved
+   beyond 2 cells, else 2.  Results agree either way (FP32 rounding). */
+#define EZMOCKB200_OPT_CIC_HALO 5
 
 int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     int *err);

@@ -98,6 +98,33 @@ def test_dens_field_fp32_error(pk_table):
     assert relmax(m.field(3), rho) <= 5e-6
 
 
+@pytest.mark.parametrize("halo", [2, 3])
+def test_dens_field_fp32_large_displacements(pk_table, halo):
+    """FP32 density with displacements of about two cells (box 100 Mpc/h on
+    64^3): many particles move beyond the assignment halo and are deposited
+    by the global-atomic pass.  Three fields in a row (the set halo, then the
+    halo the engine picks) all match the oracle."""
+    k, P = pk_table
+    m = make(32, 64, 100.0, 1, 3, k, P)
+    m.set_option(5, halo)
+    O, t, vf, psi, rho = oracle_field(64, 64, 100.0, 1, 3, k, P)
+    O32 = Oracle(32)
+    painted = None
+    for _ in range(3):
+        m.create_dens_field_from_ic()
+        assert relmax(m.field(3), rho) <= 5e-6
+        if painted is None:
+            # the oracle's painting of the GPU displacements, divided by ones
+            # (pop_tracer.c:593-683 before its division by rho)
+            psi32 = [m.field(d) for d in range(3)]
+            ones = np.ones((64, 64, 64), np.float32)
+            painted = [O32.paint(64, 100.0, psi32, ones, d) for d in range(3)]
+        for d in range(3):
+            assert relmax(m.field(4 + d), painted[d]) <= 1e-5
+    with pytest.raises(RuntimeError):
+        m.set_option(5, 4)
+
+
 @pytest.mark.parametrize("rng", [0, 1])
 def test_golden_reference_fp64(golden, pk_table, rng):
     """16^3 fields, counts and catalogue of the reference's own build."""
