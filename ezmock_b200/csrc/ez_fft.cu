@@ -431,7 +431,8 @@ wpass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0
   cplx *tw = (cplx *) smraw;
   cplx *b0 = tw + n;                         // WK lines: S, then A_0
   cplx *b1 = b0 + WK * LS;                   // WK lines: A_x
-  const int j = blockIdx.x, k0 = blockIdx.y * WK;
+  // column tiles of one j run side by side: together they read whole rows
+  const int j = blockIdx.y, k0 = blockIdx.x * WK;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
   const size_t pst = (size_t) Ng * Nkp;
@@ -489,7 +490,7 @@ wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
   cplx *bx = tw + n;                         // A_x -> B_x
   cplx *b0 = bx + WK * LS;                   // A_0 -> B_0
   cplx *by = b0 + WK * LS;                   // B_y
-  const int x = blockIdx.x, k0 = blockIdx.y * WK;
+  const int x = blockIdx.y, k0 = blockIdx.x * WK;     // tiles of one plane side by side
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
   const size_t base = (size_t) x * Ng * Nkp + k0;
@@ -801,11 +802,11 @@ int run_wpass_ij(EzMesh *m, const FftPlanDev &pn) {
   cudaFuncSetAttribute(wpass_j<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_j);
   const int nkt = (m->Nk + WK - 1) / WK;
   ez_stage_begin(m, ST_FFT_I);
-  wpass_i<E><<<dim3(Ng, nkt), 32 * WNW, sm_i, m->stream>>>(m->spec[0], m->spec[1],
+  wpass_i<E><<<dim3(nkt, Ng), 32 * WNW, sm_i, m->stream>>>(m->spec[0], m->spec[1],
       m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
   ez_stage_end(m, ST_FFT_I);
   ez_stage_begin(m, ST_FFT_J);
-  wpass_j<E><<<dim3(Ng, nkt), 32 * WNW, sm_j, m->stream>>>(m->spec[0], m->spec[1],
+  wpass_j<E><<<dim3(nkt, Ng), 32 * WNW, sm_j, m->stream>>>(m->spec[0], m->spec[1],
       m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
   ez_stage_end(m, ST_FFT_J);
   return 0;

@@ -83,7 +83,7 @@ struct EzMesh {
   int timing;              // record per-stage events
   cudaEvent_t mark[8];     // caller-placed events on the instance stream
   int cic_mode;            // 0: float atomics, 1: deterministic fixed-point
-  int cic_oh;              // halo of the owner-computes CIC (3; otherwise 2)
+  int cic_oh;              // halo of the owner-computes CIC (2; otherwise 3)
 
   int Ng;
   size_t N;                // Ng^3

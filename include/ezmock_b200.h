@@ -22,8 +22,8 @@ extern "C" {
 #define EZMOCKB200_OPT_SEED     4   /* new random seed (> 0) for the next field */
 /* Halo (2 or 3 cells) of the FP32 density assignment for the next field.
    Particles displaced farther go through a slower global-atomic pass; after
-   each field the engine picks 3 when more than 1/64 of the particles moved
-   beyond 2 cells, else 2.  Results agree either way (FP32 rounding). */
+   each field the engine picks 2 when fewer than 1/4096 of the particles
+   moved beyond 2 cells, else 3.  Results agree either way (FP32 rounding). */
 #define EZMOCKB200_OPT_CIC_HALO 5
 
 int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
