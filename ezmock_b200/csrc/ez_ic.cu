@@ -64,6 +64,29 @@ __global__ void pkq_kernel(double *__restrict__ q, int nq,
   }
 }
 
+#ifdef SINGLE_PREC
+// -log(u) for u = ez_upos(ran, x) in single precision.  For u >= 1/2 the
+// exact 1 - u is formed in integers and passed to log1p, so the result keeps
+// its relative accuracy where -log(u) is small.
+__device__ __forceinline__ float neglog_upos_f(int ran, uint32_t x) {
+  if (ran) {                                   // u = (x + 1/2) 2^-32
+    if (x < 0x80000000u) return -logf(((float) x + 0.5f) * 2.3283064365386963e-10f);
+    const uint32_t w = 0xFFFFFFFFu - x;        // 1 - u = (w + 1/2) 2^-32
+    return -log1pf(-(((float) w + 0.5f) * 2.3283064365386963e-10f));
+  }
+  // u = x / 4294967088
+  if (x < 0x80000000u) return -logf((float) x * 2.3283065e-10f);
+  const uint32_t w = 4294967088u - x;          // 1 - u = w / 4294967088
+  return -log1pf(-((float) w * 2.3283065e-10f));
+}
+
+// 2 u for u = ez_u(ran, x), the argument of sincospi for the phase 2 pi u.
+__device__ __forceinline__ float twice_u_f(int ran, uint32_t x) {
+  return ran ? (float) x * 4.656612873077393e-10f      // 2^-31
+             : (float) x * 4.656613e-10f;              // 2 / 4294967088
+}
+#endif
+
 __global__ void __launch_bounds__(IC_NT)
 ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
     const double *__restrict__ pkq, int logpk, int Ng, int Nk, int Nkp,
@@ -88,6 +111,24 @@ ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
       const bool plane = (k == 0) || (((Ng & 1) == 0) && k == Ngh);
       const size_t src = (!plane || lower) ? c : prowc + k;
       const int isq = kij + k * k;
+#ifdef SINGLE_PREC
+      // FP32 production mode: amplitude and phase in single precision from
+      // the same bit-exact draws (about 1e-7 relative per mode)
+      const float Q = (float) pkq[isq];
+      float P;
+      if (fixamp) P = logpk ? Q : sqrtf(Q);
+      else {
+        const float amp = neglog_upos_f(ran, draws[(src - 1) * per]);
+        P = logpk ? Q * sqrtf(amp) : sqrtf(Q * amp);
+      }
+      P *= (float) Pfac;
+      float sn, cs;
+      sincospif(twice_u_f(ran, draws[(src - 1) * per + per - 1]), &sn, &cs);
+      if (iphase) { sn = -sn; cs = -cs; }
+      P /= ((float) isq * (float) kfac);
+      real re = -P * sn;
+      const real im = P * cs;
+#else
       const double ksq = (double) isq;
       const double Q = pkq[isq];
       double P;
@@ -102,6 +143,7 @@ ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
       P /= (ksq * kfac);
       real re = -P * sin(phase);
       const real im = P * cos(phase);
+#endif
       if (plane && (!lower || selfp)) re = -re;
       // self-conjugate corners: (0|Ngh, 0|Ngh, 0|Ngh) except the origin
       if ((Ng & 1) == 0 && (i == 0 || i == Ngh) && (j == 0 || j == Ngh) &&
