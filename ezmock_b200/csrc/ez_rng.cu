@@ -349,8 +349,9 @@ mt_jump_kernel(uint32_t *states, const MtJumpArgs a) {
 }
 
 // Block c generates draws [c*L, min((c+1)*L, count)) from window states[c]
-// through a 1024-word ring: step g computes the 227 words 624+g .. 850+g,
-// which depend only on words g .. 623+g, so one barrier per step suffices.
+// through a 2048-word ring: step g computes the 227 words 624+g .. 850+g,
+// which depend only on words g .. 623+g; two steps run between barriers (see
+// the loop below).
 constexpr int R_THREADS = 256;
 __global__ void __launch_bounds__(R_THREADS)
 mt_ring_kernel(const uint32_t *__restrict__ states, uint64_t L, uint64_t count,
