@@ -96,8 +96,8 @@ cic_atomic_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
 // lower corner moves by at most OH cells, the upper corner lies one cell
 // above it) and likewise in y, (17 + 2 OH)^2 x 8 particles -- and keeps the
 // CIC contributions that land in its own cells, in a shared-memory ring of
-// three z chunks.  OH is 2 or 3: an instance starts with 2 and moves to 3
-// when more than 1/64 of the particles lie farther than 2 cells from their
+// three z chunks.  OH is 2 or 3: an instance starts with 3 and uses 2 while
+// fewer than 1/4096 of the particles lie farther than 2 cells from their
 // Lagrangian cell (every launch counts them).  Accumulation is in 32-bit
 // fixed point (integer shared-memory atomics are exact and fast): rho in
 // units of 2^-21 per cell, the momenta in units of 2^-s with s chosen from
@@ -423,7 +423,7 @@ int ez_cic(EzMesh *m, double Lbox) {
       }
       cudaMemsetAsync(&stats->nlist, 0, 3 * sizeof(int), m->stream);
       const unsigned nblk = (unsigned) ((Ng / OT) * (Ng / OT));
-      if (m->cic_oh == 3)
+      if (m->cic_oh != 2)
         cic_owner_kernel<3><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
             m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
       else
@@ -437,9 +437,9 @@ int ez_cic(EzMesh *m, double Lbox) {
       if (!EZ_CUDA_OK(cudaMemcpyAsync(res, &stats->overflow, sizeof(res), cudaMemcpyDeviceToHost, m->stream)) ||
           !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
         return EZMOCK_ERR_UNKNOWN;
-      // the halo for the next field of this instance: 2 while few particles
-      // move farther (they go through the global-atomic fixup)
-      m->cic_oh = ((size_t) (unsigned) res[1] > N / 64) ? 3 : 2;
+      // the halo for the next field of this instance: 2 only while almost no
+      // particle moves farther (those go through the global-atomic fixup)
+      m->cic_oh = ((size_t) (unsigned) res[1] * 4096 < N) ? 2 : 3;
       if (res[0]) {
         // a cell holds >= 1024 particles: repeat with float atomics
         cudaMemsetAsync(m->rho, 0, N * sizeof(real), m->stream);
