@@ -43,9 +43,12 @@ STAGES = ["rng", "ic", "fft_i", "fft_j", "fft_k", "cic", "bias", "select", "emit
 
 
 def workload_desc(cfg):
-    return (f"{cfg.name}: 1 mock {cfg.Ng}^3, box {cfg.Lbox:g} Mpc/h, n={cfg.n_tracer:g}, "
-            f"rho_c={cfg.rho_c:g}, rho_exp={cfg.rho_exp:g}, pdf_base={cfg.pdf_base:g}, "
-            f"sigma_v={cfg.sigma_v:g}, {'MT19937' if cfg.rng else 'MRG32k3a'}, z={cfg.z:g}")
+    pops = cfg.population_list()
+    desc = "; ".join(f"n={n:g}, rho_c={a:g}, rho_exp={e:g}, pdf_base={pb:g}, sigma_v={sv:g}"
+                     for n, a, e, pb, sv in pops)
+    return (f"{cfg.name}: 1 mock {cfg.Ng}^3, box {cfg.Lbox:g} Mpc/h, "
+            f"{len(pops)} population{'s' if len(pops) > 1 else ''} ({desc}), "
+            f"{'MT19937' if cfg.rng else 'MRG32k3a'}, z={cfg.z:g}")
 
 
 def pk_trim_len(k, Ng, Lbox):
@@ -174,7 +177,8 @@ def cpu_reference(cfg, k, P, steps, warmup, allow_scale=True):
         m.setup_pk(k, P)
         t0 = time.perf_counter()
         m.create()
-        m.populate(cfg.params(), int(round(cfg.n_tracer * Lbox ** 3)))
+        for n_t, *par in cfg.population_list():
+            m.populate(par, int(round(n_t * Lbox ** 3)))
         return time.perf_counter() - t0
 
     # a 256^3 probe decides whether full-size steps fit in a few minutes
@@ -248,8 +252,8 @@ def main():
     m.set_option(2, 1)                # stage timings
     m.eval_growth_params(cfg.z, cfg.omega_m)
     m.setup_linear_pk(k, P)
-    nexp = cfg.nexp
-    params = cfg.params()
+    # one or more populations of the same field: (nexp, [rho_c, rho_exp, pdf_base, sigma_v])
+    pops = [(int(round(n_t * cfg.Lbox ** 3)), par) for n_t, *par in cfg.population_list()]
     b = 4 if args.prec == 32 else 8
 
     def barrier():
@@ -265,8 +269,13 @@ def main():
         m.set_option(4, seed[0])
         m.create_dens_field_from_ic()
         stage_c = m.stage_times()
-        n = m.populate_device(*params, nexp)
-        return n, stage_c
+        n, stage_p = 0, {}
+        for nexp_i, par in pops:
+            n += m.populate_device(*par, nexp_i)
+            for s_, v_ in m.stage_times().items():
+                if v_ >= 0:
+                    stage_p[s_] = stage_p.get(s_, 0.0) + v_
+        return n, stage_c, stage_p
 
     clk = ClockSampler(local)
     clk.start()
@@ -280,10 +289,9 @@ def main():
     stage_acc = {s: [] for s in STAGES}
     ntr = 0
     for _ in range(args.steps):
-        ntr, st_c = device_step()
-        st_p = m.stage_times()
+        ntr, st_c, st_p = device_step()
         for s in STAGES:
-            v = st_p[s] if s not in ("rng", "ic", "fft_i", "fft_j", "fft_k", "cic") else st_c[s]
+            v = st_p.get(s, -1) if s not in ("rng", "ic", "fft_i", "fft_j", "fft_k", "cic") else st_c[s]
             if v >= 0:
                 stage_acc[s].append(v)
     L.EZmockB200_mark(m._ez, 1)
@@ -306,14 +314,17 @@ def main():
         m.set_option(4, seed[0])
         m.setup_linear_pk(k, P)               # P(k) table uploaded by the next call
         m.create_dens_field_from_ic()
-        cat = m.populate_tracer(*params, nexp)
+        n_out = 0
+        for nexp_i, par in pops:
+            cat = m.populate_tracer(*par, nexp_i)
+            n_out += len(cat[0])
     L.EZmockB200_mark(m._ez, 3)
     e2e_wall = time.perf_counter() - te0
     ems = ctypes.c_double()
     L.EZmockB200_elapsed(m._ez, 2, 3, ctypes.byref(ems))
     e2e = job_seconds_per_mock(reduce_max(max(ems.value / 1e3, e2e_wall)), n_gpus, args.steps)
     h2d = 3 * pk_trim_len(k, cfg.Ng, cfg.Lbox) * 8
-    d2h = 6 * len(cat[0]) * b
+    d2h = 6 * n_out * b
 
     # roofline of the dominant kernel
     peak, peak_kind = read_peak()
@@ -336,8 +347,11 @@ def main():
         "dtype": "f32" if args.prec == 32 else "f64",
         "data": "synthetic (BBKS P(k), sigma_8 = 0.81)",
         "config": {"workload": workload_desc(cfg), "Ngrid": cfg.Ng, "Lbox": cfg.Lbox,
-                   "nexp": nexp, "ntracer": ntr, "parallelism": f"replicas x{n_gpus}",
-                   "l2": "inputs larger than L2 (psi 1.6 GB, spectra 1.7 GB per mock)"},
+                   "nexp": pops[0][0] if len(pops) == 1 else [p_[0] for p_ in pops],
+                   "ntracer": ntr, "parallelism": f"replicas x{n_gpus}",
+                   "l2": f"inputs larger than L2 (psi {3 * cfg.Ng ** 3 * b / 1e9:.1f} GB, "
+                         f"spectra {3 * cfg.Ng ** 2 * (cfg.Ng // 2 + 1) * 2 * b / 1e9:.1f} GB "
+                         "per mock)"},
         "e2e": {"value": e2e, "unit": "s/mock", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches, "roofline": roof, "stages": stages_gbs,

@@ -422,6 +422,12 @@ constexpr int WNW = 8;                       // warps per block
 constexpr int WK = 8;                        // columns per tile (passes I, J)
 
 // pass I: A_x = FFT_i(S k_x), A_0 = FFT_i(S); one column per warp.
+// Blocks per SM the launch bounds of pass J plan for: two up to Ng = 512;
+// its 1024-point tile (197 KB of shared memory) allows one, so the register
+// budget is not halved there (no spills: 10.6 vs 12.1 ms at 1024^3).  Pass I
+// keeps two (measured faster at 1024^3 despite small spills).
+template <int E> constexpr int wpass_min_blocks() { return E >= 32 ? 1 : 2; }
+
 template <int E>
 __global__ void __launch_bounds__(32 * WNW, 2)
 wpass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0,
@@ -481,7 +487,7 @@ wpass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0
 // pass J: B_x = FFT_j(A_x) -> s1, B_y = FFT_j(A_0 k_y) -> s0,
 // B_0 = FFT_j(A_0) -> s2.
 template <int E>
-__global__ void __launch_bounds__(32 * WNW, 2)
+__global__ void __launch_bounds__(32 * WNW, wpass_min_blocks<E>())
 wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
     int Ng, int Nkp, const cplx *__restrict__ twn) {
   constexpr int n = 32 * E, LS = n + 1;

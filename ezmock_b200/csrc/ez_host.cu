@@ -164,8 +164,10 @@ void mesh_free_device(EzMesh *m) {
   if (m->side) cudaStreamDestroy(m->side);
   if (m->ev_main) cudaEventDestroy(m->ev_main);
   if (m->ev_side) cudaEventDestroy(m->ev_side);
+  if (m->ev_pop) cudaEventDestroy(m->ev_pop);
   if (m->rng_side) cudaFree(m->rng_side);
   if (m->draws_bias) cudaFree(m->draws_bias);
+  if (m->draws_pop) cudaFree(m->draws_pop);
   for (int i = 0; i < 2 * ST_NSTAGE; i++) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
   for (int i = 0; i < 8; i++) if (m->mark[i]) cudaEventDestroy(m->mark[i]);
 }
@@ -173,13 +175,14 @@ void mesh_free_device(EzMesh *m) {
 // The population stages' random streams for the instance seed (bias draws
 // 2N.., positions 5N.., dispersion 8N..; pop_tracer.c:233-237, :919, :1071),
 // prepared on the side stream while the field is created.  The position and
-// dispersion capacities are those of the last population of the instance.
+// dispersion capacities are the largest of the previous field's populations.
 void side_streams(EZMOCK *ez) {
   EzMesh *m = MESH(ez);
   const uint64_t N = m->N, h = m->pop_hint;
   const uint64_t starts[3] = {N << 1, N * 5, N << 3};
   const uint64_t caps[3] = {N + 2, 3 * h, 6 * ((h + 1) / 2)};
   ez_rng_side_prepare(m, RNG(ez)->ran, RNG(ez)->seed, starts, caps, h ? 3 : 1, N + 2);
+  m->pop_hint_reset = true;
 }
 
 void side_streams_cb(void *ez) { side_streams((EZMOCK *) ez); }

@@ -106,16 +106,21 @@ struct EzMesh {
   // side stream: the population stages' random streams for the current seed,
   // prepared while the field is being created (ez_rng_side_prepare)
   cudaStream_t side;
-  cudaEvent_t ev_main, ev_side;
+  cudaEvent_t ev_main, ev_side, ev_pop;
   uint32_t *rng_side;      // chunk states of the side ranges
   size_t rng_side_cap;     // bytes
   uint32_t *draws_bias;    // draws of side range 0 (the bias stage)
   size_t draws_bias_cap;   // uint32 values
+  uint32_t *draws_pop;     // draws of side ranges 1 and 2 (positions, dispersion)
+  size_t draws_pop_cap;    // uint32 values
   bool pre_valid;
   int pre_ran, pre_n;
   uint64_t pre_seed, pre_bias_n;
+  uint64_t pre_pop_n[2];   // draws of ranges 1, 2 generated into draws_pop (ez_rng_side_pop)
+  bool pop_pending;        // that generation may still read prepared states
   EzRange pre[3];
-  size_t pop_hint;         // tracer capacity of the last population (0: none)
+  size_t pop_hint;         // largest tracer capacity of the last field's populations
+  bool pop_hint_reset;     // the next population starts a new field's maximum
   void *est;               // clustering-estimator buffer (ez_pk.cu)
   size_t est_cap;
   void *att;               // attach-to-particle stage buffer (ez_pop.cu)
@@ -185,6 +190,7 @@ int ez_rng_draws(EzMesh *m, int ran, uint64_t seed, int i, uint64_t count,
 // work so far: chunk states of the ranges [starts[i], starts[i] + caps[i])
 // (MT19937) and the first `nbias` draws of range 0.  Failures only leave
 // the side results unused.
+void ez_rng_side_pop(EzMesh *m, int ran, uint64_t seed);
 void ez_rng_side_prepare(EzMesh *m, int ran, uint64_t seed,
     const uint64_t *starts, const uint64_t *caps, int n, uint64_t nbias);
 // Conversions shared by all kernels (prand definitions of the oracle):

@@ -1125,10 +1125,13 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   ez_stage_begin(m, ST_BIAS);
   {
     const uint64_t nt_cap = ntot + ntot / 32 + 1024;
-    m->pop_hint = nt_cap;                 // capacity for the next field's side streams
+    // capacity for the next field's side streams: the largest population
+    m->pop_hint = m->pop_hint_reset ? nt_cap : std::max<size_t>(m->pop_hint, nt_cap);
+    m->pop_hint_reset = false;
     const uint64_t starts[3] = {(uint64_t) N << 1, (uint64_t) N * 5, (uint64_t) N << 3};
     const uint64_t caps[3] = {(uint64_t) N + 2, 3 * nt_cap, 6 * ((nt_cap + 1) / 2)};
     if ((e = ez_rng_prepare(m, ran, seed, starts, caps, 3))) return e;
+    ez_rng_side_pop(m, ran, seed);
   }
 
   // ---- 1. valid ranks ----

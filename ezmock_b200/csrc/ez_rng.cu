@@ -881,6 +881,12 @@ int ez_rng_fill(EzMesh *m, int ran, uint64_t seed, uint64_t start,
 int ez_rng_prepare(EzMesh *m, int ran, uint64_t seed, const uint64_t *starts,
     const uint64_t *caps, int n) {
   m->rng_nprep = 0;
+  // the side stream's position/dispersion generation reads the states about
+  // to be replaced
+  if (m->pop_pending) {
+    if (!EZ_CUDA_OK(cudaStreamWaitEvent(m->stream, m->ev_pop, 0))) return EZMOCK_ERR_UNKNOWN;
+    m->pop_pending = false;
+  }
   if (n > EZ_RNG_MAXPREP) return EZMOCK_ERR_UNKNOWN;
   // ranges the side stream prepared for this seed and generator
   bool side[EZ_RNG_MAXPREP] = {false, false, false, false};
@@ -942,6 +948,12 @@ int ez_rng_draws(EzMesh *m, int ran, uint64_t seed, int i, uint64_t count,
     *res = m->draws_bias;                   // generated on the side stream
     return 0;
   }
+  if (prepared && (i == 1 || i == 2) && count <= m->pre_pop_n[i - 1]) {
+    // generated on the side stream at the start of the population
+    if (!EZ_CUDA_OK(cudaStreamWaitEvent(m->stream, m->ev_pop, 0))) return EZMOCK_ERR_UNKNOWN;
+    *res = m->draws_pop + (i == 2 ? m->pre_pop_n[0] : 0);
+    return 0;
+  }
   const uint64_t start = m->rng_prep[i < m->rng_nprep ? i : 0].start;
   if (ran != EZMOCK_RNG_MT19937) return mrg_fill(m, seed, start, count, out);
   if (!prepared)
@@ -958,6 +970,62 @@ int ez_rng_draws(EzMesh *m, int ran, uint64_t seed, int i, uint64_t count,
       (const uint32_t *) (m->rng_prep[i].side ? m->rng_side : m->rng_scratch), r, count, out);
 }
 
+// Side buffer for the position and dispersion draws (false: none).
+bool side_pop_buffer(EzMesh *m, uint64_t words) {
+  if (!words) return false;
+  if (words > m->draws_pop_cap) {
+    if (m->draws_pop) cudaFree(m->draws_pop);
+    m->draws_pop = nullptr;
+    m->draws_pop_cap = 0;
+    if (!EZ_CUDA_OK(cudaMalloc(&m->draws_pop, words * sizeof(uint32_t)))) {
+      cudaGetLastError();
+      return false;
+    }
+    m->draws_pop_cap = words;
+  }
+  return true;
+}
+
+// The position and dispersion ranges (prepared ranges 1 and 2 of the
+// population, at their prepared capacities) generated on the side stream while
+// the instance stream runs the bias and selection stages; ez_rng_draws makes
+// the instance stream wait for them.  Their chunks are few and long (the
+// chunk length is shared with the bias range), so on the instance stream their
+// generation would be latency on the critical path.  Launched here rather
+// than while the field is created: there they would share SMs with the CIC
+// kernel, whose shared-memory traffic starves the ring generator.
+void ez_rng_side_pop(EzMesh *m, int ran, uint64_t seed) {
+  m->pre_pop_n[0] = m->pre_pop_n[1] = 0;
+  if (m->rng_nprep < 3 || !m->side || !m->ev_pop) return;
+  const uint64_t c1 = m->rng_prep[1].cap, c2 = m->rng_prep[2].cap;
+  if (!side_pop_buffer(m, c1 + c2)) return;
+  if (!EZ_CUDA_OK(cudaEventRecord(m->ev_main, m->stream)) ||
+      !EZ_CUDA_OK(cudaStreamWaitEvent(m->side, m->ev_main, 0)))
+    return;
+  uint32_t *out[2] = {m->draws_pop, m->draws_pop + c1};
+  for (int i = 1; i <= 2; i++) {
+    const EzMesh::EzRange &p = m->rng_prep[i];
+    int e;
+    if (ran == EZMOCK_RNG_MT19937) {
+      MtRange r;
+      r.start = p.start;
+      r.cap = p.cap;
+      r.l = p.l;
+      r.P = p.P;
+      r.p = -1;
+      r.first = p.first;
+      e = mt_gen_launch(m->side, (const uint32_t *) (p.side ? m->rng_side : m->rng_scratch),
+          r, p.cap, out[i - 1]);
+    }
+    else e = mrg_fill_st(m->device, m->side, seed, p.start, p.cap, out[i - 1]);
+    if (e) return;
+  }
+  if (!EZ_CUDA_OK(cudaEventRecord(m->ev_pop, m->side))) return;
+  m->pop_pending = true;
+  m->pre_pop_n[0] = c1;
+  m->pre_pop_n[1] = c2;
+}
+
 void ez_rng_side_prepare(EzMesh *m, int ran, uint64_t seed,
     const uint64_t *starts, const uint64_t *caps, int n, uint64_t nbias) {
   m->pre_valid = false;
@@ -968,7 +1036,8 @@ void ez_rng_side_prepare(EzMesh *m, int ran, uint64_t seed,
     cudaDeviceGetStreamPriorityRange(&lo, &hi);       // lo: lowest priority
     if (!EZ_CUDA_OK(cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, lo)) ||
         !EZ_CUDA_OK(cudaEventCreateWithFlags(&m->ev_main, cudaEventDisableTiming)) ||
-        !EZ_CUDA_OK(cudaEventCreateWithFlags(&m->ev_side, cudaEventDisableTiming))) {
+        !EZ_CUDA_OK(cudaEventCreateWithFlags(&m->ev_side, cudaEventDisableTiming)) ||
+        !EZ_CUDA_OK(cudaEventCreateWithFlags(&m->ev_pop, cudaEventDisableTiming))) {
       cudaGetLastError();
       return;
     }

@@ -73,6 +73,11 @@ class MockConfig:
     def params(self):
         return [self.rho_c, self.rho_exp, self.pdf_base, self.sigma_v]
 
+    def population_list(self):
+        """(n_tracer, rho_c, rho_exp, pdf_base, sigma_v) of every population
+        drawn from one field (the base parameters when none are listed)."""
+        return [tuple(p) for p in self.populations] or [(self.n_tracer, *self.params())]
+
 
 CONFIGS = {
     # Plain EZmock at 128^3, box 1000 Mpc/h, seed 1 (parity case).
