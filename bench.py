@@ -117,6 +117,12 @@ class ClockSampler:
                 stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
+            # nvidia-smi's start-up holds the driver for up to about half a
+            # second; wait for its first sample so that this stall falls
+            # before the warm-up, not inside the timed region
+            t_end = time.perf_counter() + 10.0
+            while not self.lines and time.perf_counter() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 

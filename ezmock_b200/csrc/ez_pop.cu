@@ -197,7 +197,9 @@ bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
 // candidate list is irrelevant: it is sorted next).
 __global__ void __launch_bounds__(NT)
 compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
-    skey_t *__restrict__ keys, unsigned long long *counter) {
+    skey_t *__restrict__ keys, unsigned long long *counter, skey_t *__restrict__ cand,
+    uint16_t *__restrict__ cidx, size_t ccap, unsigned long long *__restrict__ cstart,
+    unsigned int *__restrict__ ccnt) {
   __shared__ unsigned long long sw[32];
   __shared__ unsigned long long sbase;
   const size_t b0 = (size_t) blockIdx.x * CH;
@@ -211,13 +213,23 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
   }
   unsigned long long tot;
   unsigned long long off = block_scan<unsigned long long>((unsigned long long) c, &tot, sw);
-  if (threadIdx.x == 0) sbase = tot ? atomicAdd(counter, tot) : 0;
+  if (threadIdx.x == 0) {
+    sbase = tot ? atomicAdd(counter, tot) : 0;
+    cstart[blockIdx.x] = sbase;
+    ccnt[blockIdx.x] = (unsigned int) tot;
+  }
   __syncthreads();
   off += sbase;
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    if (id < N && !(v[q] < thres)) keys[off++] = to_key(v[q]);
+    if (id < N && !(v[q] < thres)) {
+      const skey_t k = to_key(v[q]);
+      keys[off] = k;
+      // a second copy with the cell's place in the chunk, kept for emission
+      if (off < ccap) { cand[off] = k; cidx[off] = (uint16_t) (q * NT + threadIdx.x); }
+      off++;
+    }
   }
 }
 
@@ -396,6 +408,31 @@ __device__ __forceinline__ int cell_count(real v, const real *lo, const int *ntr
   return ntr[a];
 }
 
+// Tracers of a chunk from its candidates (the cells at or above the
+// selection's cut, listed by compact_kernel): only they can hold tracers.
+__global__ void __launch_bounds__(NT)
+cand_count_kernel(const skey_t *__restrict__ cand,
+    const unsigned long long *__restrict__ cstart, const unsigned int *__restrict__ ccnt,
+    const BoundOut *__restrict__ bo, unsigned long long *cnt) {
+  __shared__ real slo[EZ_MAX_NT];
+  __shared__ int sntr[EZ_MAX_NT];
+  __shared__ unsigned long long sw[32];
+  const unsigned int n = ccnt[blockIdx.x];
+  if (!n) {
+    if (threadIdx.x == 0) cnt[blockIdx.x] = 0;
+    return;
+  }
+  const int nb = bo->nbins;
+  for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
+  __syncthreads();
+  const skey_t *c = cand + cstart[blockIdx.x];
+  unsigned long long t = 0;
+  for (unsigned int i = threadIdx.x; i < n; i += NT) t += cell_count(from_key(c[i]), slo, sntr, nb);
+  unsigned long long tot;
+  block_scan<unsigned long long>(t, &tot, sw);
+  if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
+}
+
 __global__ void __launch_bounds__(NT)
 tracer_count_kernel(const real *__restrict__ rhot, size_t N,
     const BoundOut *__restrict__ bo, unsigned long long *cnt,
@@ -443,20 +480,39 @@ nt_kernel(const real *__restrict__ rhot, size_t N,
 // (skipped for the many warp rows without tracers); each tracer's cell index
 // is written to `cid`, and place_kernel computes the positions one thread per
 // tracer.
-template <typename cid_t>
+// CAND: the per-cell counts come from the chunk's candidates (cell counts
+// placed in shared memory by their place in the chunk) instead of rho_t of
+// every cell; chunks without candidates hold no tracers and return at once.
+template <typename cid_t, bool CAND>
 __global__ void __launch_bounds__(NT)
 tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
     const BoundOut *__restrict__ bo, const unsigned long long *__restrict__ off,
-    unsigned long long ntr, cid_t *__restrict__ cid, const int16_t *__restrict__ nt16) {
+    unsigned long long ntr, cid_t *__restrict__ cid, const int16_t *__restrict__ nt16,
+    const skey_t *__restrict__ cand, const uint16_t *__restrict__ cidx,
+    const unsigned long long *__restrict__ cstart, const unsigned int *__restrict__ ccnt) {
   constexpr int NW = NT / 32;
   __shared__ real slo[EZ_MAX_NT];
   __shared__ int sntr[EZ_MAX_NT];
   __shared__ unsigned int pre[ROWS * NW];
   __shared__ unsigned int wsum[ROWS * NW / 32];
+  __shared__ uint16_t lcnt[CAND ? CH : 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned int nc = 0;
+  if (CAND) {
+    nc = ccnt[blockIdx.x];
+    if (!nc) return;
+  }
   const int nb = bo->nbins;
   for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
+  if (CAND)
+    for (int e = threadIdx.x; e < CH; e += NT) lcnt[e] = 0;
   __syncthreads();
+  if (CAND) {
+    const unsigned long long c0 = cstart[blockIdx.x];
+    for (unsigned int i = threadIdx.x; i < nc; i += NT)
+      lcnt[cidx[c0 + i]] = (uint16_t) cell_count(from_key(cand[c0 + i]), slo, sntr, nb);
+    __syncthreads();
+  }
   const size_t b0 = (size_t) blockIdx.x * CH;
   int n[ROWS];
   unsigned int ex[ROWS];                       // exclusive prefix within the warp row
@@ -464,12 +520,13 @@ tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {               // all loads first
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    v[q] = (id < N && !nt16) ? rhot[id] : (real) 0;
+    v[q] = (!CAND && id < N && !nt16) ? rhot[id] : (real) 0;
   }
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    n[q] = (id < N) ? (nt16 ? (int) nt16[id] : cell_count(v[q], slo, sntr, nb)) : 0;
+    n[q] = (id >= N) ? 0 : CAND ? (int) lcnt[q * NT + threadIdx.x]
+         : (nt16 ? (int) nt16[id] : cell_count(v[q], slo, sntr, nb));
     unsigned int incl = (unsigned int) n[q];
     if (__ballot_sync(0xffffffffu, n[q] != 0)) {
 #pragma unroll
@@ -989,7 +1046,27 @@ void scan_u64(const unsigned long long *in, unsigned long long *out, size_t n,
 struct PopScratch {
   unsigned long long *bcnt, *bscan, *hist, *dpdf, *dcount, *dcscan, *counter, *tmp;
   BoundOut *bo;
+  unsigned long long *cstart;   // per chunk: first candidate (compact_kernel)
+  unsigned int *ccnt;           // per chunk: candidates
 };
+
+// Candidate copies for emission, in the draws buffer (free between the bias
+// draws and the position draws): keys, then their places in the chunk.
+struct CandBuf {
+  skey_t *key;
+  uint16_t *idx;
+  size_t cap;                   // entries
+  bool ok;                      // every candidate was copied
+};
+
+CandBuf cand_buf(EzMesh *m) {
+  CandBuf c;
+  c.cap = m->draws ? m->draws_cap * sizeof(uint32_t) / (sizeof(skey_t) + sizeof(uint16_t)) : 0;
+  c.key = (skey_t *) m->draws;
+  c.idx = (uint16_t *) ((char *) m->draws + c.cap * sizeof(skey_t));
+  c.ok = false;
+  return c;
+}
 
 int pop_scratch(EzMesh *m, PopScratch *ps) {
   const size_t N = m->N;
@@ -1005,7 +1082,9 @@ int pop_scratch(EzMesh *m, PopScratch *ps) {
   const size_t off_ctr = off_dcs + (256 * ntile_max + 1) * 8;
   const size_t off_tmp = off_ctr + 64;
   const size_t ntmp = (256 * ntile_max + nblk) / SCAN_CHUNK + 8;
-  int e = ez_scratch(m, off_tmp + ntmp * 8);
+  const size_t off_cst = off_tmp + ntmp * 8;
+  const size_t off_ccn = off_cst + nblk * 8;
+  int e = ez_scratch(m, off_ccn + nblk * 4);
   if (e) return e;
   char *sc = (char *) m->scratch;
   ps->bcnt = (unsigned long long *) (sc + off_cnt);
@@ -1017,6 +1096,8 @@ int pop_scratch(EzMesh *m, PopScratch *ps) {
   ps->dcscan = (unsigned long long *) (sc + off_dcs);
   ps->counter = (unsigned long long *) (sc + off_ctr);
   ps->tmp = (unsigned long long *) (sc + off_tmp);
+  ps->cstart = (unsigned long long *) (sc + off_cst);
+  ps->ccnt = (unsigned int *) (sc + off_ccn);
   return 0;
 }
 
@@ -1031,7 +1112,7 @@ struct HostBounds {
 // tie extension.  Leaves the boundaries in ps.bo on the device.
 int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
     const unsigned long long *h, const size_t *pdf, int nmax, size_t ncell,
-    size_t ntot, HostBounds *hb) {
+    size_t ntot, HostBounds *hb, CandBuf *cb = nullptr) {
   const size_t N = m->N;
   cudaStream_t st = m->stream;
   skey_t *keys_a = (skey_t *) m->spec[1];
@@ -1046,12 +1127,15 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
   const real cut = (imax == EZ_NLOGB - 1) ? (real) EZ_REAL_MIN
       : (real) pow(2.0, (double) ilogb_max - imax);
   cudaMemsetAsync(ps.counter, 0, 8, st);
+  CandBuf none = {nullptr, nullptr, 0, false};
+  CandBuf &c = cb ? *cb : none;
   compact_kernel<<<(unsigned) ((N + CH - 1) / CH), NT, 0, st>>>(rhot, N, cut, keys_a,
-      ps.counter); ez_count_launch();
+      ps.counter, c.key, c.idx, c.cap, ps.cstart, ps.ccnt); ez_count_launch();
   unsigned long long M = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(&M, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
     return EZMOCK_ERR_UNKNOWN;
+  c.ok = c.key && M <= c.cap;
   skey_t *sorted = keys_a;
   if (M > 1) {
     const size_t ntiles = (M + TILE - 1) / TILE;
@@ -1167,7 +1251,8 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // ---- 3. selection ----
   ez_stage_begin(m, ST_SELECT);
   HostBounds hb;
-  if ((e = select_stage(m, ps, rhot, h, pdf, nmax, ncell, ntot, &hb))) return e;
+  CandBuf cb = cand_buf(m);
+  if ((e = select_stage(m, ps, rhot, h, pdf, nmax, ncell, ntot, &hb, &cb))) return e;
   ez_stage_end(m, ST_SELECT);
   if (hb.err) { res->err = hb.err; return 0; }
   res->ncell = hb.ncell;
@@ -1252,7 +1337,14 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   }
   const size_t nrand = nt_all - iv;              // tracers at random cell positions
 
-  tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt, nt16); ez_count_launch();
+  // per-cell counts from the selection's candidates, unless attached tracers
+  // changed them (then the remaining counts are in nt16)
+  const bool usecand = !nt16 && cb.ok;
+  if (usecand)
+    cand_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(cb.key, ps.cstart, ps.ccnt, bo, bcnt);
+  else
+    tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt, nt16);
+  ez_count_launch();
   scan_u64(bcnt, bscan, nblk, ps.tmp, st);
   unsigned long long ncount = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(&ncount, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
@@ -1260,25 +1352,39 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
     return EZMOCK_ERR_UNKNOWN;
   // the per-cell counts must add up to the selected total (pop_tracer.c:989-993)
   if (ncount != nrand) { res->err = EZMOCK_ERR_UNKNOWN; return 0; }
+  // tracer cell indices in the velocity arrays (written later); before the
+  // position draws, which may reuse the draws buffer holding the candidates
+  void *cidv = (N <= 0xffffffffULL) ? (void *) (cvx + iv) : (void *) cvx;
+  if (N <= 0xffffffffULL) {
+    if (usecand)
+      tracer_cell_kernel<uint32_t, true><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
+          (unsigned long long) nrand, (uint32_t *) cidv, nt16, cb.key, cb.idx, ps.cstart, ps.ccnt);
+    else
+      tracer_cell_kernel<uint32_t, false><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
+          (unsigned long long) nrand, (uint32_t *) cidv, nt16, cb.key, cb.idx, ps.cstart, ps.ccnt);
+  }
+  else {                                            // vx and vy (iv = 0)
+    if (usecand)
+      tracer_cell_kernel<unsigned long long, true><<<(unsigned) nblk, NT, 0, st>>>(rhot, N,
+          bo, bscan, (unsigned long long) nrand, (unsigned long long *) cidv, nt16, cb.key,
+          cb.idx, ps.cstart, ps.ccnt);
+    else
+      tracer_cell_kernel<unsigned long long, false><<<(unsigned) nblk, NT, 0, st>>>(rhot, N,
+          bo, bscan, (unsigned long long) nrand, (unsigned long long *) cidv, nt16, cb.key,
+          cb.idx, ps.cstart, ps.ccnt);
+  }
+  ez_count_launch();
   if ((e = ensure_draws(m, std::max((size_t) 3 * nrand, (size_t) 1)))) return e;
   const uint32_t *dpos = nullptr;
   if ((e = ez_rng_draws(m, ran, seed, 1, 3 * nrand, m->draws, &dpos))) return e;
-  // tracer cell indices in the velocity arrays (written later)
-  if (N <= 0xffffffffULL) {
-    uint32_t *cid = (uint32_t *) (cvx + iv);
-    tracer_cell_kernel<uint32_t><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
-        (unsigned long long) nrand, cid, nt16); ez_count_launch();
-    if (nrand)
-      place_kernel<uint32_t><<<grid_for(nrand, NT), NT, 0, st>>>(cid, nrand, Ng,
-          dpos, ran, gs, Lbox, cx + iv, cy + iv, cz + iv); ez_count_launch();
-  }
-  else {
-    unsigned long long *cid = (unsigned long long *) cvx;      // vx and vy (iv = 0)
-    tracer_cell_kernel<unsigned long long><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo,
-        bscan, (unsigned long long) nrand, cid, nt16); ez_count_launch();
-    if (nrand)
-      place_kernel<unsigned long long><<<grid_for(nrand, NT), NT, 0, st>>>(cid, nrand,
-          Ng, dpos, ran, gs, Lbox, cx, cy, cz); ez_count_launch();
+  if (nrand) {
+    if (N <= 0xffffffffULL)
+      place_kernel<uint32_t><<<grid_for(nrand, NT), NT, 0, st>>>((const uint32_t *) cidv,
+          nrand, Ng, dpos, ran, gs, Lbox, cx + iv, cy + iv, cz + iv);
+    else
+      place_kernel<unsigned long long><<<grid_for(nrand, NT), NT, 0, st>>>(
+          (const unsigned long long *) cidv, nrand, Ng, dpos, ran, gs, Lbox, cx, cy, cz);
+    ez_count_launch();
   }
   ez_stage_end(m, ST_EMIT);
 

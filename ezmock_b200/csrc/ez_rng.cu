@@ -991,9 +991,7 @@ bool side_pop_buffer(EzMesh *m, uint64_t words) {
 // the instance stream runs the bias and selection stages; ez_rng_draws makes
 // the instance stream wait for them.  Their chunks are few and long (the
 // chunk length is shared with the bias range), so on the instance stream their
-// generation would be latency on the critical path.  Launched here rather
-// than while the field is created: there they would share SMs with the CIC
-// kernel, whose shared-memory traffic starves the ring generator.
+// generation would be latency on the critical path.
 void ez_rng_side_pop(EzMesh *m, int ran, uint64_t seed) {
   m->pre_pop_n[0] = m->pre_pop_n[1] = 0;
   if (m->rng_nprep < 3 || !m->side || !m->ev_pop) return;
