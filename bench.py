@@ -306,7 +306,6 @@ def main():
     wall = time.perf_counter() - t0
     launches = L.EZmockB200_launch_count() - l0
     clk.mark(t0, t0 + wall)
-    clocks = clk.stop()
     barrier()
     t_dev = reduce_max(ms.value / 1e3)
     value = job_seconds_per_mock(t_dev, n_gpus, args.steps)
@@ -329,6 +328,9 @@ def main():
     ems = ctypes.c_double()
     L.EZmockB200_elapsed(m._ez, 2, 3, ctypes.byref(ems))
     e2e = job_seconds_per_mock(reduce_max(max(ems.value / 1e3, e2e_wall)), n_gpus, args.steps)
+    # the sampler stops after every timed region (stopping nvidia-smi, like
+    # starting it, may hold the driver for a moment)
+    clocks = clk.stop()
     h2d = 3 * pk_trim_len(k, cfg.Ng, cfg.Lbox) * 8
     d2h = 6 * n_out * b
 
