@@ -200,36 +200,47 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
     skey_t *__restrict__ keys, unsigned long long *counter, skey_t *__restrict__ cand,
     uint16_t *__restrict__ cidx, size_t ccap, unsigned long long *__restrict__ cstart,
     unsigned int *__restrict__ ccnt) {
-  __shared__ unsigned long long sw[32];
+  // candidates are written warp row by warp row (ballot ranks), so each
+  // warp's stores are contiguous; their order within the chunk's range is
+  // irrelevant (the keys are sorted, the copies carry their place)
+  constexpr int NW = NT / 32;
+  __shared__ unsigned int wtot[NW];
   __shared__ unsigned long long sbase;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const size_t b0 = (size_t) blockIdx.x * CH;
   real v[ROWS];
-  unsigned int c = 0;
+  unsigned int bal[ROWS];
+  unsigned int wc = 0;
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     v[q] = (id < N) ? rhot[id] : (real) 0;
-    c += (id < N && !(v[q] < thres));
+    bal[q] = __ballot_sync(0xffffffffu, id < N && !(v[q] < thres));
+    wc += __popc(bal[q]);
   }
-  unsigned long long tot;
-  unsigned long long off = block_scan<unsigned long long>((unsigned long long) c, &tot, sw);
+  if (lane == 0) wtot[w] = wc;
+  __syncthreads();
   if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (int k = 0; k < NW; k++) tot += wtot[k];
     sbase = tot ? atomicAdd(counter, tot) : 0;
     cstart[blockIdx.x] = sbase;
     ccnt[blockIdx.x] = (unsigned int) tot;
   }
   __syncthreads();
-  off += sbase;
+  unsigned long long off = sbase;
+  for (int k = 0; k < w; k++) off += wtot[k];
+  const unsigned int lt = (1u << lane) - 1;
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
-    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    if (id < N && !(v[q] < thres)) {
+    if ((bal[q] >> lane) & 1) {
+      const unsigned long long pos = off + __popc(bal[q] & lt);
       const skey_t k = to_key(v[q]);
-      keys[off] = k;
+      keys[pos] = k;
       // a second copy with the cell's place in the chunk, kept for emission
-      if (off < ccap) { cand[off] = k; cidx[off] = (uint16_t) (q * NT + threadIdx.x); }
-      off++;
+      if (pos < ccap) { cand[pos] = k; cidx[pos] = (uint16_t) (q * NT + threadIdx.x); }
     }
+    off += __popc(bal[q]);
   }
 }
 
