@@ -610,17 +610,13 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
   }
   int nthr = CONF(ez)->nthread > 0 ? CONF(ez)->nthread : omp_get_num_procs();
   nthr = std::max(1, std::min(nthr, 8));
-  // The arrays are fresh malloc() memory: ask for huge pages and fault them
-  // in with several threads while the GPU finishes the catalogue, so the
-  // copy-out below runs at memcpy speed.
+  // The arrays may be fresh malloc() memory: fault them in with several
+  // threads while the GPU finishes the catalogue, so the copy-out below runs
+  // at memcpy speed.  (No huge-page advice: where the kernel compacts memory
+  // synchronously for advised regions, a fault stalled for up to a second.)
   const size_t bytes_arr = n * sizeof(real);
   if (bytes_arr >= ((size_t) 4 << 20)) {
     const size_t pg = 4096, npg = (bytes_arr + pg - 1) / pg;
-    for (int a = 0; a < 6; a++) {
-      const uintptr_t b = ((uintptr_t) cat[a] + pg - 1) & ~(uintptr_t) (pg - 1);
-      const uintptr_t e = ((uintptr_t) cat[a] + bytes_arr) & ~(uintptr_t) (pg - 1);
-      if (e > b) madvise((void *) b, e - b, MADV_HUGEPAGE);
-    }
 #pragma omp parallel for num_threads(nthr) schedule(static)
     for (long p = 0; p < (long) (6 * npg); p++)
       ((volatile char *) cat[p / npg])[(p % npg) * pg] = 0;
