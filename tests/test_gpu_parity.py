@@ -20,6 +20,7 @@ import pytest
 
 from ezmock_b200 import EZmock, _lib
 from ezmock_b200.workloads import wiggle_pk
+from oracle import pkest
 from oracle.pyoracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -193,6 +194,39 @@ def test_populate_fp64(pk_table, rng, params, n):
     vmax = np.abs(np.stack(ref[3:])).max()
     for a in range(3, 6):
         assert np.abs(cat[a] - ref[a]).max() <= 1e-9 * vmax
+
+
+def test_populate_fp32_against_fp64_oracle(pk_table):
+    """The FP32 mode against the FP64 oracle on the benchmark's cell size and
+    tracer density (64^3, box 312.5 Mpc/h): the FP32 field error moves no
+    cell across rho_c, so the valid-cell ranks that index the bias Gaussians
+    (pop_tracer.c:233-237) are the same, and every cell gets the same number
+    of tracers; P0 and P2 (40 bins, 0.005-0.3 h/Mpc, RSD) agree within 0.5%
+    of P0.  (Where the error moves a cell across rho_c, the Gaussians of
+    every later valid cell shift, in the reference's own FP32 build as
+    here.)"""
+    k, P = pk_table
+    Ng, L, seed = 64, 312.5, 7
+    params = [0.8, 20.0, 0.3, 400.0]
+    nexp = int(round(2e-4 * L ** 3))
+    m = make(32, Ng, L, 1, seed, k, P)
+    m.create_dens_field_from_ic()
+    cat = m.populate_tracer(*params, nexp)
+    O, t, vf, psi, rho = oracle_field(64, Ng, L, 1, seed, k, P)
+    e, ref = O.populate(Ng, L, 1, seed, vf, psi, rho, params, nexp)
+    assert e == 0
+    rho32 = m.field(3)
+    assert relmax(rho32, rho) <= 5e-6
+    # the precondition: the same valid cells (float and double comparisons)
+    assert np.array_equal(rho32 >= np.float32(params[0]), rho >= params[0])
+    assert np.array_equal(cell_counts(*cat[:3], Ng, L), cell_counts(*ref[:3], Ng, L))
+    rsd = 0.0114
+    p32 = pkest.powspec(*cat[:3], L, 64, True, 0.005, 0.3, 40, vz=cat[5], rsd_fac=rsd)
+    p64 = pkest.powspec(*ref[:3], L, 64, True, 0.005, 0.3, 40, vz=ref[5], rsd_fac=rsd)
+    has = p64["nmodes"] > 0
+    scale = np.abs(p64["P0"])[has]
+    assert np.all(np.abs(p32["P0"] - p64["P0"])[has] <= 5e-3 * scale)
+    assert np.all(np.abs(p32["P2"] - p64["P2"])[has] <= 5e-3 * scale)
 
 
 def test_populate_fp32_positions(pk_table):
