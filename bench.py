@@ -97,77 +97,113 @@ def read_traffic(workload):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples while the timed region runs."""
+    """SM clock and throttle-reason samples, every 200 ms, while the timed
+    region runs: read in this process through NVML (three calls per sample),
+    or, where NVML cannot be loaded, from an `nvidia-smi -lms 200` process."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.proc = None
-        self.lines = []                 # (host time, csv line)
+        self.nvml = None
+        self.samples = []               # (host time, sm MHz, max MHz, reason names)
         self.window = None
+        self.done = threading.Event()
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+            self.nvml = (pynvml, h)
+            self.bits = [pynvml.nvmlClocksEventReasonHwSlowdown,
+                         pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                         pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                         pynvml.nvmlClocksEventReasonSwPowerCap]
+            self.th = threading.Thread(target=self._poll, daemon=True)
+            self.th.start()
+        except Exception:
+            self.nvml = None
+            self._start_smi()
+        # the first sample before the warm-up: start-up stays out of the timed
+        # region
+        t_end = time.perf_counter() + 10.0
+        while not self.samples and time.perf_counter() < t_end and \
+                (self.nvml is not None or (self.proc and self.proc.poll() is None)):
+            time.sleep(0.01)
+
+    def _poll(self):
+        nv, h = self.nvml
+        while not self.done.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), float(sm), float(mx),
+                                     [n for n, b in zip(self.NAMES, self.bits) if r & b]))
+            except Exception:
+                pass
+            self.done.wait(0.2)
+
+    def _start_smi(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                  "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL, text=True)
-            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th = threading.Thread(target=self._read_smi, daemon=True)
             self.th.start()
-            # nvidia-smi's start-up holds the driver for up to about half a
-            # second; wait for its first sample so that this stall falls
-            # before the warm-up, not inside the timed region
-            t_end = time.perf_counter() + 10.0
-            while not self.lines and time.perf_counter() < t_end and self.proc.poll() is None:
-                time.sleep(0.01)
         except Exception:
             self.proc = None
 
-    def _read(self):
+    def _read_smi(self):
         for line in self.proc.stdout:
-            self.lines.append((time.perf_counter(), line.strip()))
-
-    def mark(self, t0, t1):
-        """Keep only samples taken between host times t0 and t1 (the timed
-        region); the sampler itself starts before the warm-up so that its
-        start-up does not fall inside the timed region."""
-        self.window = (t0, t1)
-
-    def stop(self):
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.th.join(timeout=2)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        lines = [ln for t, ln in self.lines
-                 if self.window is None or self.window[0] <= t <= self.window[1]]
-        if not lines and self.lines:     # timed region shorter than one period
-            t_mid = 0.5 * (self.window[0] + self.window[1])
-            lines = [min(self.lines, key=lambda x: abs(x[0] - t_mid))[1]]
-        for ln in lines:
-            p = [x.strip() for x in ln.split(",")]
+            p = [x.strip() for x in line.strip().split(",")]
             if len(p) < 9:
                 continue
             try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
+                self.samples.append((time.perf_counter(), float(p[1]), float(p[2]),
+                                     [n for n, v in zip(self.NAMES, p[5:9])
+                                      if v.lower() == "active"]))
             except ValueError:
                 continue
-            for nm, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+
+    def mark(self, t0, t1):
+        """Keep only samples taken between host times t0 and t1 (the timed
+        region)."""
+        self.window = (t0, t1)
+
+    def stop(self):
+        self.done.set()
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.nvml is None and not self.proc:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        self.th.join(timeout=2)
+        if self.nvml is not None:
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
+        sel = [x for x in self.samples
+               if self.window is None or self.window[0] <= x[0] <= self.window[1]]
+        if not sel and self.samples:     # timed region shorter than one period
+            t_mid = 0.5 * (self.window[0] + self.window[1])
+            sel = [min(self.samples, key=lambda x: abs(x[0] - t_mid))]
+        if not sel:
+            return None
+        reasons = sorted({n for x in sel for n in x[3]})
+        return {"sm_mhz": statistics.median(x[1] for x in sel), "sm_max_mhz": sel[-1][2],
+                "reasons": reasons, "samples": len(sel),
+                "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 def cpu_reference(cfg, k, P, steps, warmup, allow_scale=True):
@@ -328,8 +364,7 @@ def main():
     ems = ctypes.c_double()
     L.EZmockB200_elapsed(m._ez, 2, 3, ctypes.byref(ems))
     e2e = job_seconds_per_mock(reduce_max(max(ems.value / 1e3, e2e_wall)), n_gpus, args.steps)
-    # the sampler stops after every timed region (stopping nvidia-smi, like
-    # starting it, may hold the driver for a moment)
+    # the sampler stops after every timed region
     clocks = clk.stop()
     h2d = 3 * pk_trim_len(k, cfg.Ng, cfg.Lbox) * 8
     d2h = 6 * n_out * b

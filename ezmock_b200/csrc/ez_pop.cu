@@ -306,59 +306,58 @@ digit_hist_kernel(const skey_t *__restrict__ keys, size_t M, int shift,
   counts[(size_t) threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// Scatter of one tile by the digit at `shift`, stable: key i of the tile
+// goes to the tile's start of its digit (offs, from the digit counts of all
+// tiles) plus the number of keys with the same digit before it in the tile.
+// Warp w takes tile positions w*32*PER + j*32 + lane (j = 0 .. PER-1, in
+// order); a key's rank among equal digits comes from __match_any_sync, the
+// warp's running count per digit and, after the loop, the counts of the
+// warps before it.
 __global__ void __launch_bounds__(SORT_NT)
 digit_scatter_kernel(const skey_t *__restrict__ in, skey_t *__restrict__ out,
     size_t M, int shift, const unsigned long long *__restrict__ offs,
     size_t ntiles) {
-  __shared__ skey_t sk[TILE];
-  __shared__ unsigned int sw[32];
-  __shared__ unsigned int dstart[256];
+  constexpr int NW = SORT_NT / 32;
+  static_assert(SORT_NT == 256, "one thread per digit");
+  __shared__ unsigned int cnt[NW][256];
+  __shared__ unsigned long long base[256];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < NW * 256; e += SORT_NT) (&cnt[0][0])[e] = 0;
+  base[threadIdx.x] = offs[(size_t) threadIdx.x * ntiles + blockIdx.x];
+  __syncthreads();
   const size_t t0 = (size_t) blockIdx.x * TILE;
-  const int n = (int) min((size_t) TILE, M - t0);
-  // thread t holds keys at tile positions t*PER .. t*PER+PER-1
+  const unsigned int lt = (1u << lane) - 1;
   skey_t k[SORT_PER];
+  unsigned int r[SORT_PER];
+  int dg[SORT_PER];
 #pragma unroll
   for (int j = 0; j < SORT_PER; j++) {
-    const int pos = threadIdx.x * SORT_PER + j;
-    k[j] = (pos < n) ? in[t0 + pos] : ~(skey_t) 0;
+    const size_t g = t0 + (size_t) (w * 32 * SORT_PER + j * 32 + lane);
+    const bool valid = g < M;
+    k[j] = valid ? in[g] : (skey_t) 0;
+    const int d = valid ? (int) ((k[j] >> shift) & 255) : 256;   // 256: no key
+    const unsigned int mask = __match_any_sync(0xffffffffu, d);
+    r[j] = valid ? cnt[w][d] + __popc(mask & lt) : 0;
+    __syncwarp();
+    if (valid && !(mask & lt)) cnt[w][d] += __popc(mask);          // lowest lane
+    __syncwarp();
+    dg[j] = d;
   }
-  // stable sort of the tile by the 8-bit digit: eight 1-bit splits
-  for (int b = 0; b < 8; b++) {
-    unsigned int zeros = 0;
+  __syncthreads();
+  {                                      // counts of the warps before each warp
+    const int d = threadIdx.x;
+    unsigned int run = 0;
 #pragma unroll
-    for (int j = 0; j < SORT_PER; j++) zeros += !((k[j] >> (shift + b)) & 1);
-    unsigned int tz;
-    unsigned int zb = block_scan<unsigned int>(zeros, &tz, sw);
-    unsigned int ob = threadIdx.x * SORT_PER - zb;
-#pragma unroll
-    for (int j = 0; j < SORT_PER; j++) {
-      const bool one = (k[j] >> (shift + b)) & 1;
-      const unsigned int dst = one ? tz + ob++ : zb++;
-      sk[dst] = k[j];
+    for (int v = 0; v < NW; v++) {
+      const unsigned int c = cnt[v][d];
+      cnt[v][d] = run;
+      run += c;
     }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < SORT_PER; j++) k[j] = sk[threadIdx.x * SORT_PER + j];
-    __syncthreads();
-  }
-  // local start of each digit (padding keys have digit 255 and sort last)
-  dstart[threadIdx.x] = 0xffffffffu;
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < SORT_PER; j++) {
-    const int pos = threadIdx.x * SORT_PER + j;
-    const int d = (int) ((k[j] >> shift) & 255);
-    const int dprev = pos ? (int) ((sk[pos - 1] >> shift) & 255) : -1;
-    if (pos < n && d != dprev) dstart[d] = pos;
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < SORT_PER; j++) {
-    const int pos = threadIdx.x * SORT_PER + j;
-    if (pos >= n) continue;
-    const int d = (int) ((k[j] >> shift) & 255);
-    out[offs[(size_t) d * ntiles + blockIdx.x] + (pos - dstart[d])] = k[j];
-  }
+  for (int j = 0; j < SORT_PER; j++)
+    if (dg[j] < 256) out[base[dg[j]] + cnt[w][dg[j]] + r[j]] = k[j];
 }
 
 // ---- boundaries of the PDF bins (one thread; pop_tracer.c:405-461) ----
@@ -1273,11 +1272,15 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // ---- 4. emission ----
   ez_stage_begin(m, ST_EMIT);
   if (nt_all > m->cat_cap) {
+    // with slack: the tie extension varies the count by a few tracers from
+    // one field to the next, and a reallocation (cudaFree synchronises the
+    // device) cost 45-500 ms
+    const size_t cap = nt_all + nt_all / 32 + 4096;
     if (m->cat) cudaFree(m->cat);
     m->cat = nullptr;
     m->cat_cap = 0;
-    if (!EZ_CUDA_OK(cudaMalloc(&m->cat, 6 * nt_all * sizeof(real)))) return EZMOCK_ERR_MEMORY;
-    m->cat_cap = nt_all;
+    if (!EZ_CUDA_OK(cudaMalloc(&m->cat, 6 * cap * sizeof(real)))) return EZMOCK_ERR_MEMORY;
+    m->cat_cap = cap;
   }
   m->cat_n = nt_all;
   real *cx = m->cat, *cy = cx + nt_all, *cz = cy + nt_all;
