@@ -243,8 +243,6 @@ __device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
 // window extended by HW words, two MT_N result buffers, one polynomial.
 constexpr size_t H_SMEM_WORDS = (size_t) HG * HTAB * MT_N + 3 * MT_N + HW;
 constexpr size_t H_SMEM = H_SMEM_WORDS * sizeof(uint32_t);
-constexpr size_t HJ_SMEM = (H_SMEM_WORDS + (H_SMEM_WORDS & 1)) * sizeof(uint32_t) +
-    MT_PW * sizeof(uint64_t);
 
 // Applies p(T) to the window held in ext[0, MT_N) (logical order), in place.
 // Horner's rule runs over 16-bit windows of p: r <- T^16 r + sum_g
@@ -316,8 +314,8 @@ mt_horner_kernel(uint32_t *states, const int4 *__restrict__ desc,
 }
 
 // Direct jumps of up to four ranges from one seed window, passed by value
-// (no host-to-device copy, hence no stream synchronisation): block b of range
-// i computes chunk c = b - (blocks of earlier ranges) and writes
+// (no host-to-device copy, hence no stream synchronisation): chunk g of the
+// launch (range i, chunk c = g - chunks of earlier ranges) is written to
 // states[first[i] + c] = (poly[i] + c MT_PW)(T) seed.
 constexpr int MT_MAXR = 4;
 struct MtJumpArgs {
@@ -328,24 +326,82 @@ struct MtJumpArgs {
   const uint64_t *poly[MT_MAXR];             // P polynomials each
 };
 
+// Direct jumps, two chunks per block: both come from the one seed window,
+// so they share its tables, and Horner's rule advances both states in each
+// window with one barrier.  The per-window chain of shared-memory reads and
+// a barrier is what bounds a jump, so two chunks per block take about the
+// time of one, and a launch of up to 296 chunks fits one block per SM.
+constexpr size_t HJ2_SMEM_WORDS = (size_t) HG * HTAB * MT_N + MT_N + HW + 4 * MT_N;
+constexpr size_t HJ2_SMEM = (HJ2_SMEM_WORDS + (HJ2_SMEM_WORDS & 1)) * sizeof(uint32_t) +
+    2 * MT_PW * sizeof(uint64_t);
+
 __global__ void __launch_bounds__(H_THREADS)
-mt_jump_kernel(uint32_t *states, const MtJumpArgs a) {
+mt_jump2_kernel(uint32_t *states, const MtJumpArgs a, int nst) {
   extern __shared__ uint32_t sm[];
-  int i = 0, c = blockIdx.x;
-  while (i < a.nr - 1 && c >= a.P[i]) { c -= a.P[i]; i++; }
-  const uint64_t *poly = a.poly[i] + (size_t) c * MT_PW;
-  uint32_t *tab = sm;
-  uint32_t *ext = tab + HG * HTAB * MT_N;
-  uint32_t *ra = ext + MT_N + HW;
-  uint32_t *rb = ra + MT_N;
-  uint64_t *pp = (uint64_t *) (sm + H_SMEM_WORDS + (H_SMEM_WORDS & 1));
+  uint32_t *tab = sm;                         // HG x HTAB x MT_N
+  uint32_t *ext = tab + HG * HTAB * MT_N;     // seed window + HW words
+  uint32_t *ra0 = ext + MT_N + HW, *ra1 = ra0 + MT_N;   // chunk A states
+  uint32_t *rb0 = ra1 + MT_N, *rb1 = rb0 + MT_N;        // chunk B states
+  uint64_t *pp = (uint64_t *) (sm + HJ2_SMEM_WORDS + (HJ2_SMEM_WORDS & 1));
   const int t = threadIdx.x;
+  const int g0 = 2 * blockIdx.x;
+  const bool two = g0 + 1 < nst;
+  const uint64_t *poly[2] = {nullptr, nullptr};
+  uint32_t *dst[2] = {nullptr, nullptr};
+  for (int h = 0; h < (two ? 2 : 1); h++) {
+    int i = 0, c = g0 + h;
+    while (i < a.nr - 1 && c >= a.P[i]) { c -= a.P[i]; i++; }
+    poly[h] = a.poly[i] + (size_t) c * MT_PW;
+    dst[h] = states + (size_t) (a.first[i] + c) * MT_N;
+  }
   for (int k = t; k < MT_N; k += blockDim.x) ext[k] = a.w[k];
-  for (int k = t; k < MT_PW; k += blockDim.x) pp[k] = poly[k];
+  for (int k = t; k < MT_PW; k += blockDim.x) {
+    pp[k] = poly[0][k];
+    pp[MT_PW + k] = two ? poly[1][k] : 0;
+  }
   __syncthreads();
-  horner_apply(ext, tab, ra, rb, pp);
-  uint32_t *dst = states + (size_t) (a.first[i] + c) * MT_N;
-  for (int k = t; k < MT_N; k += blockDim.x) dst[k] = ext[k];
+  if (t < HW) ext[MT_N + t] = mt_f(ext[t], ext[t + 1], ext[MT_M + t]);
+  __syncthreads();
+  for (int e = t; e < HG * HTAB * MT_N; e += blockDim.x) {
+    const int gc = e / MT_N, k = e - gc * MT_N;
+    const int g = gc / HTAB, c = gc - g * HTAB;
+    uint32_t v = 0;
+#pragma unroll
+    for (int j = 0; j < HSUB; j++)
+      if (c & (1 << j)) v ^= ext[k + HSUB * g + j];
+    tab[e] = v;
+  }
+  for (int k = t; k < 2 * MT_N; k += blockDim.x) { ra0[k] = 0; rb0[k] = 0; }
+  __syncthreads();
+  const int nwin = (MT_DEG + HW - 1) / HW;
+  for (int q = nwin - 1; q >= 0; q--) {
+    const int b = q * HW;                      // HW = 16 divides 64
+    const uint32_t ba = (uint32_t) (pp[b >> 6] >> (b & 63)) & 0xffffu;
+    const uint32_t bb = (uint32_t) (pp[MT_PW + (b >> 6)] >> (b & 63)) & 0xffffu;
+    if (t < MT_N) {
+      uint32_t va, vb;
+      if (t < MT_N - HW) { va = ra0[t + HW]; vb = rb0[t + HW]; }
+      else {
+        const int s = t - (MT_N - HW);
+        va = mt_f(ra0[s], ra0[s + 1], ra0[MT_M + s]);
+        vb = mt_f(rb0[s], rb0[s + 1], rb0[MT_M + s]);
+      }
+#pragma unroll
+      for (int g = 0; g < HG; g++) {
+        va ^= tab[(g * HTAB + ((ba >> (HSUB * g)) & (HTAB - 1))) * MT_N + t];
+        vb ^= tab[(g * HTAB + ((bb >> (HSUB * g)) & (HTAB - 1))) * MT_N + t];
+      }
+      ra1[t] = va;
+      rb1[t] = vb;
+    }
+    __syncthreads();
+    uint32_t *x = ra0; ra0 = ra1; ra1 = x;
+    x = rb0; rb0 = rb1; rb1 = x;
+  }
+  for (int k = t; k < MT_N; k += blockDim.x) {
+    dst[0][k] = ra0[k];
+    if (two) dst[1][k] = rb0[k];
+  }
 }
 
 // Block c generates draws [c*L, min((c+1)*L, count)) from window states[c]
@@ -554,8 +610,8 @@ int mt_prepare(int dev) {
   if (!EZ_CUDA_OK(cudaFuncSetAttribute(mt_horner_kernel,
           cudaFuncAttributeMaxDynamicSharedMemorySize,
           (int) H_SMEM)) ||
-      !EZ_CUDA_OK(cudaFuncSetAttribute(mt_jump_kernel,
-          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) HJ_SMEM)))
+      !EZ_CUDA_OK(cudaFuncSetAttribute(mt_jump2_kernel,
+          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) HJ2_SMEM)))
     return EZMOCK_ERR_UNKNOWN;
   g_mt_dev_ready = dev;
   return 0;
@@ -773,7 +829,8 @@ int mt_jump_launch(int dev, cudaStream_t st, uint32_t *states, uint64_t seed,
   }
   if (!nst) return 0;
   mt_seed_window(seed, a.w);
-  mt_jump_kernel<<<(unsigned) nst, H_THREADS, HJ_SMEM, st>>>(states, a); ez_count_launch();
+  mt_jump2_kernel<<<(unsigned) ((nst + 1) / 2), H_THREADS, HJ2_SMEM, st>>>(states, a, (int) nst);
+  ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
