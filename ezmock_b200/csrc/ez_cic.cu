@@ -106,8 +106,10 @@ cic_atomic_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
 // plain coalesced stores, so every output cell is written exactly once and
 // no global atomics are needed.  Particles displaced by more than OH cells in
 // any direction are listed by their own CTA and deposited afterwards with
-// global atomics (fixup_kernel).  A negative rho sum (overflow) raises a flag
-// on which the host repeats the assignment with float atomics.
+// global atomics (fixup_kernel).  No in-kernel sum can overflow: a cell is
+// reached only by particles within OH + 1 Lagrangian cells on each axis,
+// (2 OH + 2)^3 <= 512 of them, each with weight <= 1, so rho < 2^9 and the
+// momenta stay below 512 max|psi| scale <= 2^30.
 constexpr int OT = 16;                       // owned column tile (x and y)
 constexpr int OKZ = 8;                       // z slices per chunk
 constexpr int ORS = 3 * OKZ;                 // ring: three chunks
@@ -280,8 +282,6 @@ cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
         src[0] = make_int4(0, 0, 0, 0);
         src[1] = make_int4(0, 0, 0, 0);
         const float f = (q == 0) ? (1.f / RHO_SCALE) : minv;
-        if (q == 0 && (va.x | va.y | va.z | va.w | vb.x | vb.y | vb.z | vb.w) < 0)
-          stats->overflow = 1;
         real *g = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
         const int cx = col / OT, cy = col - cx * OT;
         float4 *dst = reinterpret_cast<float4 *>(
@@ -421,7 +421,12 @@ int ez_cic(EzMesh *m, double Lbox) {
         cudaMemsetAsync(&stats->psimax_bits, 0, sizeof(unsigned int), m->stream);
         psi_absmax_kernel<<<148 * 8, 256, 0, m->stream>>>(m->psi[0], 3 * N, stats); ez_count_launch();
       }
-      cudaMemsetAsync(&stats->nlist, 0, 3 * sizeof(int), m->stream);
+      // the halo: set by the caller, else from the previous field's count if
+      // it has arrived
+      if (m->cic_oh_set) m->cic_oh_set = false;
+      else if (m->h_cic && cudaEventQuery(m->ev_cic) == cudaSuccess)
+        m->cic_oh = ((size_t) m->h_cic[0] * 4096 < N) ? 2 : 3;
+      cudaMemsetAsync(&stats->nlist, 0, 2 * sizeof(int), m->stream);
       const unsigned nblk = (unsigned) ((Ng / OT) * (Ng / OT));
       if (m->cic_oh != 2)
         cic_owner_kernel<3><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
@@ -433,20 +438,20 @@ int ez_cic(EzMesh *m, double Lbox) {
       fixup_kernel<<<148 * 4, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
           m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs,
           stats, list); ez_count_launch();
-      int res[2] = {0, 0};                            // overflow, nfar2
-      if (!EZ_CUDA_OK(cudaMemcpyAsync(res, &stats->overflow, sizeof(res), cudaMemcpyDeviceToHost, m->stream)) ||
-          !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
-        return EZMOCK_ERR_UNKNOWN;
-      // the halo for the next field of this instance: 2 only while almost no
-      // particle moves farther (those go through the global-atomic fixup)
-      m->cic_oh = ((size_t) (unsigned) res[1] * 4096 < N) ? 2 : 3;
-      if (res[0]) {
-        // a cell holds >= 1024 particles: repeat with float atomics
-        cudaMemsetAsync(m->rho, 0, N * sizeof(real), m->stream);
-        for (int d = 0; d < 3; d++) cudaMemsetAsync(m->paint[d], 0, N * sizeof(real), m->stream);
-        cic_atomic_kernel<true><<<grid, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
-            m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, N); ez_count_launch();
+      // this field's count of particles beyond 2 cells, for the next field's
+      // halo (2 only while almost none move farther; those take the
+      // global-atomic fixup); read into pinned memory without waiting
+      if (!m->h_cic) {
+        if (!EZ_CUDA_OK(cudaMallocHost(&m->h_cic, sizeof(unsigned int))) ||
+            !EZ_CUDA_OK(cudaEventCreateWithFlags(&m->ev_cic, cudaEventDisableTiming))) {
+          m->h_cic = nullptr;
+          return EZMOCK_ERR_MEMORY;
+        }
       }
+      if (!EZ_CUDA_OK(cudaMemcpyAsync(m->h_cic, &stats->nfar2, sizeof(unsigned int),
+              cudaMemcpyDeviceToHost, m->stream)) ||
+          !EZ_CUDA_OK(cudaEventRecord(m->ev_cic, m->stream)))
+        return EZMOCK_ERR_UNKNOWN;
     }
     else
 #endif

@@ -159,6 +159,8 @@ void mesh_free_device(EzMesh *m) {
   if (m->cat) cudaFree(m->cat);
   if (m->h_stage) cudaFreeHost(m->h_stage);
   if (m->h_small) cudaFreeHost(m->h_small);
+  if (m->h_cic) cudaFreeHost(m->h_cic);
+  if (m->ev_cic) cudaEventDestroy(m->ev_cic);
   for (int i = 0; i < 2; i++) if (m->d2h_ev[i]) cudaEventDestroy(m->d2h_ev[i]);
   if (m->stream) cudaStreamDestroy(m->stream);
   if (m->side) cudaStreamDestroy(m->side);
@@ -861,6 +863,7 @@ int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     case EZMOCKB200_OPT_CIC_HALO:
       if (value != 2 && value != 3) return (*err = EZMOCK_ERR_ARG_PARAMS);
       m->cic_oh = (int) value;
+      m->cic_oh_set = true;               // not replaced by the last field's count
       return 0;
     default: return (*err = EZMOCK_ERR_ARG_PARAMS);
   }

@@ -84,6 +84,7 @@ struct EzMesh {
   cudaEvent_t mark[8];     // caller-placed events on the instance stream
   int cic_mode;            // 0: float atomics, 1: deterministic fixed-point
   int cic_oh;              // halo of the owner-computes CIC (2; otherwise 3)
+  bool cic_oh_set;         // cic_oh set by the caller for the next field
 
   int Ng;
   size_t N;                // Ng^3
@@ -134,6 +135,8 @@ struct EzMesh {
   size_t cat_n;            // length of the last catalogue (array stride)
   real *h_stage;           // pinned host staging for the catalogue
   unsigned long long *h_small;  // pinned host staging for small uploads (EZ_MAX_NT words)
+  unsigned int *h_cic;     // pinned: the last CIC's nfar2, read without waiting
+  cudaEvent_t ev_cic;      // h_cic written
   size_t h_stage_cap;
   cudaEvent_t d2h_ev[2];   // staging halves ready
 };
@@ -142,8 +145,8 @@ struct EzMesh {
 struct EzCicStats {
   unsigned int psimax_bits;   // max |psi| over the three fields (float bits)
   unsigned int nlist;         // far-displaced particles listed for fixup
-  int overflow;               // a fixed-point cell sum overflowed
   unsigned int nfar2;         // particles displaced by more than 2 cells on some axis
+  int pad;
 };
 
 // ---- error helpers ----

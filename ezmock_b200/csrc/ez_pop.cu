@@ -110,8 +110,10 @@ scan_kernel(const unsigned long long *__restrict__ in, unsigned long long *out,
 // uses the cosine, 2p+1 the sine.  The multiplicative factor
 // G = 1 + g (g >= 0) or exp(g) (pop_tracer.c:288-300) is stored per rank.
 __global__ void __launch_bounds__(NT)
-gauss_pair_kernel(const uint32_t *__restrict__ draws, size_t npair, int ran,
-    double lambda, double *__restrict__ G) {
+gauss_pair_kernel(const uint32_t *__restrict__ draws,
+    const unsigned long long *__restrict__ nvalid, int ran, double lambda,
+    double *__restrict__ G) {
+  const size_t npair = (size_t) ((*nvalid + 1) >> 1);   // pairs for the valid cells
   for (size_t p = (size_t) blockIdx.x * NT + threadIdx.x; p < npair;
        p += (size_t) gridDim.x * NT) {
     const double rr = -2 * log(ez_upos(ran, draws[2 * p]));
@@ -1231,31 +1233,29 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // ---- 1. valid ranks ----
   valid_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, N, thres, bcnt); ez_count_launch();
   scan_u64(bcnt, bscan, nblk, ps.tmp, st);
-  unsigned long long nvalid = 0;
-  if (!EZ_CUDA_OK(cudaMemcpyAsync(&nvalid, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
+
+  // ---- 2. bias ----
+  // The valid count stays on the device until the histogram is read: the
+  // draws cover every cell (the side stream prepared N + 2 of them), the
+  // Box-Muller pairs stop at the count.
+  const size_t nd_max = N + (N & 1);
+  if ((e = ensure_draws(m, std::max(nd_max, (size_t) 1)))) return e;
+  const uint32_t *dbias = nullptr;
+  if ((e = ez_rng_draws(m, ran, seed, 0, nd_max, m->draws, &dbias))) return e;
+  cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
+  // G per valid rank in spec[1..2] (free until the selection's sort)
+  double *G = (double *) m->spec[1];
+  gauss_pair_kernel<<<grid_for(nd_max / 2, NT), NT, 0, st>>>(dbias, bscan + nblk, ran,
+      (double) (real) EZ_GAUSS_WIDTH, G); ez_count_launch();
+  bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
+      bscan, G, hist); ez_count_launch();
+  unsigned long long h[EZ_NLOGB], nvalid = 0;
+  if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaMemcpyAsync(&nvalid, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
     return EZMOCK_ERR_UNKNOWN;
   res->nvalid = nvalid;
   if (nvalid < ncell) { res->err = EZMOCK_ERR_RHO_LESS; return 0; }
-
-  // ---- 2. bias ----
-  const size_t nd_bias = nvalid + (nvalid & 1);
-  if ((e = ensure_draws(m, std::max(nd_bias, (size_t) 1)))) return e;
-  const uint32_t *dbias = nullptr;
-  if ((e = ez_rng_draws(m, ran, seed, 0, nd_bias, m->draws, &dbias))) return e;
-  cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
-  // G per valid rank in spec[1..2] (free until the selection's sort)
-  double *G = (double *) m->spec[1];
-  const size_t npair = nd_bias / 2;
-  if (npair)
-    gauss_pair_kernel<<<grid_for(npair, NT), NT, 0, st>>>(dbias, npair, ran,
-        (double) (real) EZ_GAUSS_WIDTH, G); ez_count_launch();
-  bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
-      bscan, G, hist); ez_count_launch();
-  unsigned long long h[EZ_NLOGB];
-  if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
-      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
-    return EZMOCK_ERR_UNKNOWN;
   ez_stage_end(m, ST_BIAS);
 
   // ---- 3. selection ----
