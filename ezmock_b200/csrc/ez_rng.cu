@@ -15,17 +15,18 @@
 //  * MT19937 (Matsumoto & Nishimura 1998): the 624-word window of the stream
 //    at any offset J is p(T) applied to the seed window, p = x^J mod phi
 //    (Haramoto et al. 2008).  phi is found once on the host by
-//    Berlekamp-Massey and the table x^(2^k) mod phi by repeated squaring.  On
-//    the GPU one block applies p(T) with Horner's rule over 16-bit windows
-//    (four 16-entry tables of combinations of T^j s held in shared memory,
-//    one barrier per window).  Chunk c of a range [start, start + P*L) is
-//    reached directly from the seed window with x^(start + c L) mod phi; the
-//    host computes these polynomials once per (start, L) with carry-less
-//    products (ez_gf2.cpp) and keeps them on the device, so all P chunk
-//    states come from one launch.  Each chunk is then generated by one block
-//    through a ring buffer, 227 words per barrier.  (Without the host
-//    arithmetic the states are built by one jump to `start` and log2(P)
-//    doubling levels, the scheme the allocation-free entry point uses.)
+//    Berlekamp-Massey and the table x^(2^k) mod phi by repeated squaring.
+//    Chunk c of a range [start, start + P*L) is reached directly from the
+//    seed window with x^(start + c L) mod phi; the host computes these
+//    polynomials once per (start, L) with carry-less products (ez_gf2.cpp)
+//    and keeps them on the device.  Since T^b s is the stream's window at b,
+//    p(T) s is a convolution of p's bits with the first 20k words of the
+//    stream: all chunk states of a launch come from one barrier-free pass
+//    over 4-bit tables (mt_jumpd_kernel).  Each chunk is then generated by
+//    one block through a ring buffer, 227 words per barrier.  (Without the
+//    host arithmetic the states are built with Horner's rule over 16-bit
+//    windows, by one jump to `start` and log2(P) doubling levels, the scheme
+//    the allocation-free entry point uses.)
 #include "ez_internal.cuh"
 #include "ezmock_b200.h"
 #include "ez_gf2.h"
@@ -326,81 +327,130 @@ struct MtJumpArgs {
   const uint64_t *poly[MT_MAXR];             // P polynomials each
 };
 
-// Direct jumps, two chunks per block: both come from the one seed window,
-// so they share its tables, and Horner's rule advances both states in each
-// window with one barrier.  The per-window chain of shared-memory reads and
-// a barrier is what bounds a jump, so two chunks per block take about the
-// time of one, and a launch of up to 296 chunks fits one block per SM.
-constexpr size_t HJ2_SMEM_WORDS = (size_t) HG * HTAB * MT_N + MT_N + HW + 4 * MT_N;
-constexpr size_t HJ2_SMEM = (HJ2_SMEM_WORDS + (HJ2_SMEM_WORDS & 1)) * sizeof(uint32_t) +
-    2 * MT_PW * sizeof(uint64_t);
+// Direct jumps as one convolution.  With x_0, x_1, ... the raw stream from
+// the seed window (x_0 .. x_623 the window, x_n = f(x_{n-624}, x_{n-623},
+// x_{n-227})), the window T^b s is x_b .. x_{b+623}, so word w of p(T) s is
+// the XOR of x_{b+w} over the set bits b of p.  Every (chunk, word) is
+// independent: no barrier chain, unlike Horner's rule.  The bits of p are
+// taken four at a time through 16-row tables tab[v][o] = XOR of x_{o+j} over
+// the set bits j of v (built per slice of 64 nibbles from the stream in
+// global memory).  In a warp the lanes are 32 chunks and every lane adds
+// the same 48 words w, so a lane's nibble selects its row and the row stride
+// 897 = 1 (mod 32) keeps the lanes on distinct banks (equal nibbles read
+// the same word).  A block covers all 624 words for 32 chunks and one
+// segment of the polynomial; the segments' partial windows are combined by
+// atomic XOR into zeroed states, through shared memory so that the atomics
+// are coalesced.
+constexpr int JD_QB = 64;                          // nibbles per table slice
+constexpr int JD_OSV = 4 * JD_QB + MT_N;           // table columns used
+constexpr int JD_OS = 897;                         // row stride, 1 (mod 32)
+constexpr int JD_WT = 48;                          // words per thread
+constexpr int JD_THREADS = 32 * (MT_N / JD_WT);    // 13 warps
+constexpr int JD_NQ = (MT_DEG + 3) / 4;            // nibbles of p
+constexpr int JD_N8 = (JD_NQ + 7) / 8;             // 32-bit words of p read
+constexpr int JD_XL = 20832;                       // stream words read
+constexpr int JD_TP = 337;                         // transpose row stride
+constexpr int JD_HALF = 7 * JD_WT;                 // words of the first half
+constexpr size_t JD_SMEM = (size_t) 16 * JD_OS * sizeof(uint32_t);
+static_assert(JD_OS >= JD_OSV && JD_OS % 32 == 1, "table stride");
+static_assert(JD_XL >= 4 * (JD_N8 * 8 - 8) + JD_OSV + 3, "stream length");
+static_assert(32 * JD_TP <= 16 * JD_OS && JD_TP >= JD_HALF && JD_TP % 2 == 1, "transpose");
+static_assert(JD_HALF < MT_N && MT_N - JD_HALF <= JD_TP && MT_N % JD_WT == 0, "halves");
+static_assert(JD_N8 <= 2 * MT_PW, "polynomial words");
 
-__global__ void __launch_bounds__(H_THREADS)
-mt_jump2_kernel(uint32_t *states, const MtJumpArgs a, int nst) {
-  extern __shared__ uint32_t sm[];
-  uint32_t *tab = sm;                         // HG x HTAB x MT_N
-  uint32_t *ext = tab + HG * HTAB * MT_N;     // seed window + HW words
-  uint32_t *ra0 = ext + MT_N + HW, *ra1 = ra0 + MT_N;   // chunk A states
-  uint32_t *rb0 = ra1 + MT_N, *rb1 = rb0 + MT_N;        // chunk B states
-  uint64_t *pp = (uint64_t *) (sm + HJ2_SMEM_WORDS + (HJ2_SMEM_WORDS & 1));
+// x_0 .. x_{JD_XL-1} of the stream from the seed window a.w.
+constexpr int JD_SEQ_THREADS = 256;
+__global__ void __launch_bounds__(JD_SEQ_THREADS)
+mt_seq_kernel(const MtJumpArgs a, uint32_t *__restrict__ xs) {
+  extern __shared__ uint32_t sx[];                 // JD_XL words
   const int t = threadIdx.x;
-  const int g0 = 2 * blockIdx.x;
-  const bool two = g0 + 1 < nst;
-  const uint64_t *poly[2] = {nullptr, nullptr};
-  uint32_t *dst[2] = {nullptr, nullptr};
-  for (int h = 0; h < (two ? 2 : 1); h++) {
-    int i = 0, c = g0 + h;
-    while (i < a.nr - 1 && c >= a.P[i]) { c -= a.P[i]; i++; }
-    poly[h] = a.poly[i] + (size_t) c * MT_PW;
-    dst[h] = states + (size_t) (a.first[i] + c) * MT_N;
-  }
-  for (int k = t; k < MT_N; k += blockDim.x) ext[k] = a.w[k];
-  for (int k = t; k < MT_PW; k += blockDim.x) {
-    pp[k] = poly[0][k];
-    pp[MT_PW + k] = two ? poly[1][k] : 0;
-  }
+  for (int k = t; k < MT_N; k += JD_SEQ_THREADS) sx[k] = a.w[k];
   __syncthreads();
-  if (t < HW) ext[MT_N + t] = mt_f(ext[t], ext[t + 1], ext[MT_M + t]);
-  __syncthreads();
-  for (int e = t; e < HG * HTAB * MT_N; e += blockDim.x) {
-    const int gc = e / MT_N, k = e - gc * MT_N;
-    const int g = gc / HTAB, c = gc - g * HTAB;
-    uint32_t v = 0;
+  constexpr int S = MT_N - MT_M;                   // 227 words per step
+  for (int n0 = MT_N; n0 < JD_XL; n0 += S) {
+    const int n = n0 + t;
+    if (t < S && n < JD_XL) sx[n] = mt_f(sx[n - MT_N], sx[n - MT_N + 1], sx[n - S]);
+    __syncthreads();
+  }
+  for (int k = t; k < JD_XL; k += JD_SEQ_THREADS) xs[k] = sx[k];
+}
+
+// Block (segment, group): chunks 32 group + lane of the launch, polynomial
+// words [8 seg JD_N8 / nseg, ...) (a multiple of 8 nibbles each).  The
+// states of the launch's chunks must be zero.
+__global__ void __launch_bounds__(JD_THREADS, 2)
+mt_jumpd_kernel(uint32_t *states, const MtJumpArgs a, int nst, int nseg,
+    const uint32_t *__restrict__ xs) {
+  extern __shared__ uint32_t tab[];                // 16 x JD_OS
+  __shared__ uint32_t pws[(JD_QB / 8) * 32];       // slice words, [k][lane]
+  __shared__ uint32_t *sdst[32];
+  const int lane = threadIdx.x & 31, w0 = (threadIdx.x >> 5) * JD_WT;
+  const int seg = blockIdx.x, grp = blockIdx.y;
+  const int qa = 8 * (int) ((long) seg * JD_N8 / nseg);
+  const int qb = 8 * (int) ((long) (seg + 1) * JD_N8 / nseg);
+  const uint32_t *poly = nullptr;
+  if (threadIdx.x < 32) {
+    uint32_t *dst = nullptr;
+    const int g = grp * 32 + lane;
+    if (g < nst) {
+      int i = 0, c = g;
+      while (i < a.nr - 1 && c >= a.P[i]) { c -= a.P[i]; i++; }
+      poly = (const uint32_t *) (a.poly[i] + (size_t) c * MT_PW);
+      dst = states + (size_t) (a.first[i] + c) * MT_N;
+    }
+    sdst[lane] = dst;
+  }
+  uint32_t acc[JD_WT];
 #pragma unroll
-    for (int j = 0; j < HSUB; j++)
-      if (c & (1 << j)) v ^= ext[k + HSUB * g + j];
-    tab[e] = v;
-  }
-  for (int k = t; k < 2 * MT_N; k += blockDim.x) { ra0[k] = 0; rb0[k] = 0; }
-  __syncthreads();
-  const int nwin = (MT_DEG + HW - 1) / HW;
-  for (int q = nwin - 1; q >= 0; q--) {
-    const int b = q * HW;                      // HW = 16 divides 64
-    const uint32_t ba = (uint32_t) (pp[b >> 6] >> (b & 63)) & 0xffffu;
-    const uint32_t bb = (uint32_t) (pp[MT_PW + (b >> 6)] >> (b & 63)) & 0xffffu;
-    if (t < MT_N) {
-      uint32_t va, vb;
-      if (t < MT_N - HW) { va = ra0[t + HW]; vb = rb0[t + HW]; }
-      else {
-        const int s = t - (MT_N - HW);
-        va = mt_f(ra0[s], ra0[s + 1], ra0[MT_M + s]);
-        vb = mt_f(rb0[s], rb0[s + 1], rb0[MT_M + s]);
-      }
-#pragma unroll
-      for (int g = 0; g < HG; g++) {
-        va ^= tab[(g * HTAB + ((ba >> (HSUB * g)) & (HTAB - 1))) * MT_N + t];
-        vb ^= tab[(g * HTAB + ((bb >> (HSUB * g)) & (HTAB - 1))) * MT_N + t];
-      }
-      ra1[t] = va;
-      rb1[t] = vb;
+  for (int i = 0; i < JD_WT; i++) acc[i] = 0;
+  for (int qs = qa; qs < qb; qs += JD_QB) {
+    const int nk = min(JD_QB, qb - qs) >> 3;       // words of p in the slice
+    __syncthreads();                               // the previous slice is read
+    if (threadIdx.x < 32)
+      for (int k = 0; k < JD_QB / 8; k++)
+        pws[k * 32 + lane] = (poly && k < nk) ? poly[(qs >> 3) + k] : 0u;
+    for (int o = threadIdx.x; o < JD_OSV; o += JD_THREADS) {
+      const uint32_t *xp = xs + 4 * qs + o;
+      const uint32_t x0 = xp[0], x1 = xp[1], x2 = xp[2], x3 = xp[3];
+      const uint32_t t01 = x0 ^ x1, t23 = x2 ^ x3;
+      uint32_t *col = tab + o;
+      col[0 * JD_OS] = 0;               col[1 * JD_OS] = x0;
+      col[2 * JD_OS] = x1;              col[3 * JD_OS] = t01;
+      col[4 * JD_OS] = x2;              col[5 * JD_OS] = x0 ^ x2;
+      col[6 * JD_OS] = x1 ^ x2;         col[7 * JD_OS] = t01 ^ x2;
+      col[8 * JD_OS] = x3;              col[9 * JD_OS] = x0 ^ x3;
+      col[10 * JD_OS] = x1 ^ x3;        col[11 * JD_OS] = t01 ^ x3;
+      col[12 * JD_OS] = t23;            col[13 * JD_OS] = x0 ^ t23;
+      col[14 * JD_OS] = x1 ^ t23;       col[15 * JD_OS] = t01 ^ t23;
     }
     __syncthreads();
-    uint32_t *x = ra0; ra0 = ra1; ra1 = x;
-    x = rb0; rb0 = rb1; rb1 = x;
+    for (int k = 0; k < nk; k++) {
+      const uint32_t p = pws[k * 32 + lane];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint32_t *tp = tab + ((p >> (4 * j)) & 15u) * JD_OS + 4 * (8 * k + j) + w0;
+#pragma unroll
+        for (int i = 0; i < JD_WT; i++) acc[i] ^= tp[i];
+      }
+    }
   }
-  for (int k = t; k < MT_N; k += blockDim.x) {
-    dst[0][k] = ra0[k];
-    if (two) dst[1][k] = rb0[k];
+  // partial windows to the states, half the words at a time
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int wlo = h ? JD_HALF : 0, whi = h ? MT_N : JD_HALF;
+    __syncthreads();
+    if (w0 >= wlo && w0 < whi) {
+#pragma unroll
+      for (int i = 0; i < JD_WT; i++) tab[lane * JD_TP + (w0 - wlo) + i] = acc[i];
+    }
+    __syncthreads();
+    const int nw = whi - wlo;
+    const int nc = min(32, nst - grp * 32);
+    for (int e = threadIdx.x; e < nc * nw; e += JD_THREADS) {
+      const int c = e / nw, w = e - c * nw;
+      const uint32_t v = tab[c * JD_TP + w];
+      if (v) atomicXor(sdst[c] + wlo + w, v);
+    }
   }
 }
 
@@ -595,6 +645,7 @@ std::mutex g_mt_mu;
 MtTables g_mt;
 bool g_mt_built = false;
 int g_mt_dev_ready = -1;
+int g_mt_nsm = 148;                          // SMs of the prepared device
 uint64_t *g_mt_xpow_dev = nullptr;
 
 int mt_prepare(int dev) {
@@ -610,8 +661,11 @@ int mt_prepare(int dev) {
   if (!EZ_CUDA_OK(cudaFuncSetAttribute(mt_horner_kernel,
           cudaFuncAttributeMaxDynamicSharedMemorySize,
           (int) H_SMEM)) ||
-      !EZ_CUDA_OK(cudaFuncSetAttribute(mt_jump2_kernel,
-          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) HJ2_SMEM)))
+      !EZ_CUDA_OK(cudaFuncSetAttribute(mt_seq_kernel,
+          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (JD_XL * sizeof(uint32_t)))) ||
+      !EZ_CUDA_OK(cudaFuncSetAttribute(mt_jumpd_kernel,
+          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) JD_SMEM)) ||
+      !EZ_CUDA_OK(cudaDeviceGetAttribute(&g_mt_nsm, cudaDevAttrMultiProcessorCount, dev)))
     return EZMOCK_ERR_UNKNOWN;
   g_mt_dev_ready = dev;
   return 0;
@@ -721,7 +775,9 @@ int mt_prepare_ranges(EzMesh *m, uint64_t seed, MtRange *r, int nr,
 // products reduced modulo phi, ez_gf2.cpp) and keeps them on the device;
 // every fill then needs one Horner pass per chunk, all chunks in one launch,
 // instead of a jump followed by log2(chunks) dependent doubling levels.
-constexpr int MT_CHUNKS = 296;              // two waves of jump blocks
+// Chunks per fill: two per SM.  (Measured at 512^3: 592 or 1184 chunks
+// cost more in jumps than the shorter chunks save in generation.)
+constexpr int MT_CHUNKS = 296;
 
 bool g_gf2_tried = false, g_gf2_ok = false;
 
@@ -829,15 +885,26 @@ int mt_jump_launch(int dev, cudaStream_t st, uint32_t *states, uint64_t seed,
   }
   if (!nst) return 0;
   mt_seed_window(seed, a.w);
-  mt_jump2_kernel<<<(unsigned) ((nst + 1) / 2), H_THREADS, HJ2_SMEM, st>>>(states, a, (int) nst);
+  // the stream words after the states; two blocks per SM in one wave
+  uint32_t *xs = states + (base + nst) * MT_N;
+  const int ncg = (int) ((nst + 31) / 32);
+  const int nseg = std::max(1, std::min(JD_N8, 2 * g_mt_nsm / ncg));
+  if (!EZ_CUDA_OK(cudaMemsetAsync(states + base * MT_N, 0, nst * MT_N * sizeof(uint32_t), st)))
+    return EZMOCK_ERR_UNKNOWN;
+  mt_seq_kernel<<<1, JD_SEQ_THREADS, JD_XL * sizeof(uint32_t), st>>>(a, xs);
+  ez_count_launch();
+  mt_jumpd_kernel<<<dim3((unsigned) nseg, (unsigned) ncg), JD_THREADS, JD_SMEM, st>>>(
+      states, a, (int) nst, nseg, xs);
   ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
+// States (624 words each) a launch of `nr` ranges needs from `base`, with
+// the stream words of the direct jumps after them.
 size_t mt_states_needed(const MtRange *r, int nr, size_t base) {
   size_t n = base;
   for (int i = 0; i < nr; i++) n += (size_t) r[i].P;
-  return n;
+  return n + (JD_XL + MT_N - 1) / MT_N;
 }
 
 int mt_prepare_direct(EzMesh *m, uint64_t seed, MtRange *r, int nr, size_t base) {
