@@ -139,6 +139,11 @@ struct EzMesh {
   cudaEvent_t ev_cic;      // h_cic written
   size_t h_stage_cap;
   cudaEvent_t d2h_ev[2];   // staging halves ready
+  cudaStream_t cpy;        // catalogue copy-out
+  cudaEvent_t ev_pos;      // positions of the catalogue final (ez_populate)
+  cudaEvent_t ev_cat;      // whole catalogue final
+  void *hpool;             // pre-faulted host blocks for catalogues (ez_host.cu)
+  long hpool_mib;          // bytes the pool may hold, MiB (0: default; < 0: off)
 };
 
 // Device-side statistics of the displacement/density assignment.

@@ -1401,6 +1401,8 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
     ez_count_launch();
   }
   ez_stage_end(m, ST_EMIT);
+  // the positions are final: their copy-out may overlap the velocities
+  if (m->ev_pos && !EZ_CUDA_OK(cudaEventRecord(m->ev_pos, st))) return EZMOCK_ERR_UNKNOWN;
 
   // ---- 5./6. velocities and dispersion ----
   ez_stage_begin(m, ST_VEL);

@@ -25,6 +25,10 @@ extern "C" {
    each field the engine picks 2 when fewer than 1/4096 of the particles
    moved beyond 2 cells, else 3.  Results agree either way (FP32 rounding). */
 #define EZMOCKB200_OPT_CIC_HALO 5
+/* Host memory (MiB) that EZmock_populate_tracer may keep in pre-faulted
+   malloc() blocks for the next catalogues (a worker thread faults them in
+   while the GPU computes); 0 turns the pool off.  Default 2048. */
+#define EZMOCKB200_OPT_HOST_POOL 6
 
 int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     int *err);

@@ -266,6 +266,33 @@ def test_repeated_populations_fp64(pk_table):
             assert np.array_equal(cat[a], ref[a])
 
 
+def test_catalogue_host_pool(pk_table):
+    """Catalogues of over 4 MB per array come from pre-faulted host blocks
+    (EZMOCKB200_OPT_HOST_POOL): repeated populations of one field give the
+    same catalogue with the pool filled, with a second population size in
+    between, and with the pool turned off."""
+    k, P = pk_table
+    Ng, L = 128, 1000.0
+    m = make(32, Ng, L, 1, 5, k, P)
+    m.create_dens_field_from_ic()
+    params = [0.3, 10.0, 0.3, 300.0]
+    nexp = 1_200_000
+    first = m.populate_tracer(*params, nexp)
+    assert len(first[0]) >= nexp
+    for n2 in (nexp, 600_000, nexp):
+        cat = m.populate_tracer(*params, n2)
+        if n2 == nexp:
+            for a in range(6):
+                assert np.array_equal(cat[a], first[a])
+    m.set_option(6, 0)
+    cat = m.populate_tracer(*params, nexp)
+    for a in range(6):
+        assert np.array_equal(cat[a], first[a])
+    m.set_option(6, 64)
+    with pytest.raises(RuntimeError):
+        m.set_option(6, -1)
+
+
 def test_white_noise_fp64(pk_table):
     k, P = pk_table
     Ng, L = 32, 250.0
