@@ -119,7 +119,9 @@ gauss_pair_kernel(const uint32_t *__restrict__ draws,
     const double rr = -2 * log(ez_upos(ran, draws[2 * p]));
     const double th = ez_u(ran, draws[2 * p + 1]) * 2 * EZ_PI;
     const double s = lambda * sqrt(rr);
-    const double g0 = s * cos(th), g1 = s * sin(th);
+    double sn, cs;
+    sincos(th, &sn, &cs);                     // one argument reduction for both
+    const double g0 = s * cs, g1 = s * sn;
     G[2 * p] = (g0 >= 0) ? 1 + g0 : exp(g0);
     G[2 * p + 1] = (g1 >= 0) ? 1 + g1 : exp(g1);
   }
