@@ -164,7 +164,7 @@ void mesh_free_device(EzMesh *m) {
   if (m->h_small) cudaFreeHost(m->h_small);
   if (m->h_cic) cudaFreeHost(m->h_cic);
   if (m->ev_cic) cudaEventDestroy(m->ev_cic);
-  for (int i = 0; i < 2; i++) if (m->d2h_ev[i]) cudaEventDestroy(m->d2h_ev[i]);
+  for (int i = 0; i < 4; i++) if (m->d2h_ev[i]) cudaEventDestroy(m->d2h_ev[i]);
   if (m->cpy) cudaStreamDestroy(m->cpy);
   if (m->ev_pos) cudaEventDestroy(m->ev_pos);
   if (m->ev_cat) cudaEventDestroy(m->ev_cat);
@@ -742,27 +742,30 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
     for (long p = 0; p < (long) (6 * npg); p++)
       if (fresh[p / npg]) ((volatile char *) cat[p / npg])[(p % npg) * pg] = 0;
   }
-  // device -> pinned staging (two 8 MB halves, DMA of one overlapping the
-  // copy-out of the other) -> the caller's malloc() arrays, copied out by
-  // several host threads.  The copies run on their own stream: the positions
-  // once they are final, while the GPU computes the velocities.
+  // device -> pinned staging (a ring of three 16 MB buffers: the DMA of the
+  // next pieces overlaps the copy-out of this one) -> the caller's malloc()
+  // arrays, copied out by up to eight host threads.  The copies run on their
+  // own stream: the positions once they are final, while the GPU computes
+  // the velocities.  (512^3, 75 MB: the copy-out after the GPU work took
+  // 2.26 ms with two 8 MB buffers and four threads, 1.85 with three, 1.49
+  // with three and six threads, 1.18 with three 16 MB buffers and eight
+  // threads; 32 MB pieces or four buffers no better.)
   ez_stage_begin(m, ST_D2H);
-  const size_t half = (size_t) 8 << 20;
-  if (m->h_stage_cap < 2 * half) {
+  const size_t piece = (size_t) 16 << 20;
+  constexpr int NB = 3;
+  if (m->h_stage_cap < NB * piece) {
     if (m->h_stage) cudaFreeHost(m->h_stage);
     m->h_stage = nullptr;
     m->h_stage_cap = 0;
-    if (!EZ_CUDA_OK(cudaMallocHost(&m->h_stage, 2 * half))) {
+    if (!EZ_CUDA_OK(cudaMallocHost(&m->h_stage, NB * piece))) {
       for (int j = 0; j < 6; j++) free(cat[j]);
       return (*err = EZMOCK_ERR_MEMORY);
     }
-    m->h_stage_cap = 2 * half;
+    m->h_stage_cap = NB * piece;
   }
-  if (!m->d2h_ev[0]) {
-    cudaEventCreateWithFlags(&m->d2h_ev[0], cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&m->d2h_ev[1], cudaEventDisableTiming);
-  }
-  const size_t per = half / sizeof(real);               // reals per half
+  for (int i = 0; i < NB; i++)
+    if (!m->d2h_ev[i]) cudaEventCreateWithFlags(&m->d2h_ev[i], cudaEventDisableTiming);
+  const size_t per = piece / sizeof(real);              // reals per piece
   struct Piece { int arr; size_t off, len; };
   std::vector<Piece> pieces;
   for (int a = 0; a < 6; a++)
@@ -770,29 +773,23 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
   bool ok = true;
   auto issue = [&](size_t k) {
     const Piece &pc = pieces[k];
-    real *stage = (real *) ((char *) m->h_stage + (k & 1) * half);
+    real *stage = (real *) ((char *) m->h_stage + (k % NB) * piece);
     if (k == 0 || pc.arr != pieces[k - 1].arr) {
       // each array waits for the kernel that completes it
       ok = ok && EZ_CUDA_OK(cudaStreamWaitEvent(m->cpy, pc.arr < 3 ? m->ev_pos : m->ev_cat, 0));
     }
     ok = ok && EZ_CUDA_OK(cudaMemcpyAsync(stage, m->cat + (size_t) pc.arr * n + pc.off,
         pc.len * sizeof(real), cudaMemcpyDeviceToHost, m->cpy));
-    ok = ok && EZ_CUDA_OK(cudaEventRecord(m->d2h_ev[k & 1], m->cpy));
+    ok = ok && EZ_CUDA_OK(cudaEventRecord(m->d2h_ev[k % NB], m->cpy));
   };
-  if (!pieces.empty()) issue(0);
+  for (size_t k = 0; k < pieces.size() && k < (size_t) NB; k++) issue(k);
   for (size_t k = 0; k < pieces.size() && ok; k++) {
-    if (k + 1 < pieces.size()) {
-      // the other half is free once its previous copy-out has finished
-      issue(k + 1);
-    }
-    ok = ok && EZ_CUDA_OK(cudaEventSynchronize(m->d2h_ev[k & 1]));
+    ok = ok && EZ_CUDA_OK(cudaEventSynchronize(m->d2h_ev[k % NB]));
     const Piece &pc = pieces[k];
-    const char *src = (const char *) m->h_stage + (k & 1) * half;
+    const char *src = (const char *) m->h_stage + (k % NB) * piece;
     char *dst = (char *) (cat[pc.arr] + pc.off);
     const size_t nb = pc.len * sizeof(real);
-    // four threads: pinned-to-pageable copies measured 15.5, 43.9, 29.7 GB/s
-    // with 1, 4 and 8 threads (the DMA runs at 51 GB/s)
-    const int nt = (nb >= ((size_t) 1 << 20)) ? std::min(nthr, 4) : 1;
+    const int nt = (nb >= ((size_t) 1 << 20)) ? nthr : 1;
     if (nt == 1) memcpy(dst, src, nb);
     else {
       const size_t step = (nb + nt - 1) / nt;
@@ -802,10 +799,12 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
         if (b1 > b0) memcpy(dst + b0, src + b0, b1 - b0);
       }
     }
+    // this buffer is free again
+    if (k + NB < pieces.size()) issue(k + NB);
   }
   // later work of the instance stream (the next catalogue) follows the copies
   if (ok && !pieces.empty())
-    ok = EZ_CUDA_OK(cudaStreamWaitEvent(m->stream, m->d2h_ev[(pieces.size() - 1) & 1], 0));
+    ok = EZ_CUDA_OK(cudaStreamWaitEvent(m->stream, m->d2h_ev[(pieces.size() - 1) % NB], 0));
   if (!ok) {
     for (int j = 0; j < 6; j++) free(cat[j]);
     return (*err = EZMOCK_ERR_UNKNOWN);

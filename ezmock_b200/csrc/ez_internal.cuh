@@ -138,7 +138,7 @@ struct EzMesh {
   unsigned int *h_cic;     // pinned: the last CIC's nfar2, read without waiting
   cudaEvent_t ev_cic;      // h_cic written
   size_t h_stage_cap;
-  cudaEvent_t d2h_ev[2];   // staging halves ready
+  cudaEvent_t d2h_ev[4];   // staging buffers ready
   cudaStream_t cpy;        // catalogue copy-out
   cudaEvent_t ev_pos;      // positions of the catalogue final (ez_populate)
   cudaEvent_t ev_cat;      // whole catalogue final
