@@ -90,7 +90,9 @@ valid_count_kernel(const real *__restrict__ rho, size_t N, real thres,
   if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
 }
 
-// single-block exclusive scan of n values; out[n] = total
+// single-block exclusive scan of n values; out[n] = total.  Each thread's
+// segment is read in batches of eight independent loads (a loop of single
+// loads was a chain of L2 latencies).
 __global__ void __launch_bounds__(1024)
 scan_kernel(const unsigned long long *__restrict__ in, unsigned long long *out,
     size_t n) {
@@ -98,10 +100,23 @@ scan_kernel(const unsigned long long *__restrict__ in, unsigned long long *out,
   const size_t per = (n + blockDim.x - 1) / blockDim.x;
   const size_t s0 = threadIdx.x * per, s1 = min(n, s0 + per);
   unsigned long long loc = 0;
-  for (size_t i = s0; i < s1; i++) loc += in[i];
+  for (size_t b = s0; b < s1; b += 8) {
+    unsigned long long v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) v[u] = (b + u < s1) ? in[b + u] : 0ull;
+#pragma unroll
+    for (int u = 0; u < 8; u++) loc += v[u];
+  }
   unsigned long long tot;
   unsigned long long run = block_scan<unsigned long long>(loc, &tot, sw);
-  for (size_t i = s0; i < s1; i++) { const unsigned long long v = in[i]; out[i] = run; run += v; }
+  for (size_t b = s0; b < s1; b += 8) {
+    unsigned long long v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) v[u] = (b + u < s1) ? in[b + u] : 0ull;
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+      if (b + u < s1) { out[b + u] = run; run += v[u]; }
+  }
   if (threadIdx.x == 0) out[n] = tot;
 }
 
@@ -374,7 +389,18 @@ struct BoundOut {
   unsigned long long pdf[EZ_MAX_NT];
 };
 
+// First index in [lo, hi) of the ascending keys with a[i] > v.  The bins'
+// boundaries rarely fall inside a run of ties, so the search gallops from
+// lo (one load when a[lo] > v already) before bisecting: a chain of
+// dependent global loads is the cost of this single-thread kernel.
 __device__ size_t upper_bound_key(const skey_t *a, size_t lo, size_t hi, skey_t v) {
+  size_t step = 1, base = lo;
+  while (base < hi && a[base] <= v) {
+    lo = base + 1;
+    base = lo + step - 1 < hi ? lo + step - 1 : hi;
+    step <<= 1;
+  }
+  hi = base;                                 // a[hi] > v, or hi is the end
   while (lo < hi) {
     const size_t mid = (lo + hi) >> 1;
     if (a[mid] <= v) lo = mid + 1; else hi = mid;
