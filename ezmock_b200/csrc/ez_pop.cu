@@ -519,40 +519,22 @@ nt_kernel(const real *__restrict__ rhot, size_t N,
 // cell comes from the chunk offset, per-(row, warp) prefixes and a warp scan
 // (skipped for the many warp rows without tracers); each tracer's cell index
 // is written to `cid`, and place_kernel computes the positions one thread per
-// tracer.
-// CAND: the per-cell counts come from the chunk's candidates (cell counts
-// placed in shared memory by their place in the chunk) instead of rho_t of
-// every cell; chunks without candidates hold no tracers and return at once.
-template <typename cid_t, bool CAND>
+// tracer.  (With the selection's candidates at hand, tracer_cell_cand_kernel
+// visits only them.)
+template <typename cid_t>
 __global__ void __launch_bounds__(NT)
 tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
     const BoundOut *__restrict__ bo, const unsigned long long *__restrict__ off,
-    unsigned long long ntr, cid_t *__restrict__ cid, const int16_t *__restrict__ nt16,
-    const skey_t *__restrict__ cand, const uint16_t *__restrict__ cidx,
-    const unsigned long long *__restrict__ cstart, const unsigned int *__restrict__ ccnt) {
+    unsigned long long ntr, cid_t *__restrict__ cid, const int16_t *__restrict__ nt16) {
   constexpr int NW = NT / 32;
   __shared__ real slo[EZ_MAX_NT];
   __shared__ int sntr[EZ_MAX_NT];
   __shared__ unsigned int pre[ROWS * NW];
   __shared__ unsigned int wsum[ROWS * NW / 32];
-  __shared__ uint16_t lcnt[CAND ? CH : 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  unsigned int nc = 0;
-  if (CAND) {
-    nc = ccnt[blockIdx.x];
-    if (!nc) return;
-  }
   const int nb = bo->nbins;
   for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
-  if (CAND)
-    for (int e = threadIdx.x; e < CH; e += NT) lcnt[e] = 0;
   __syncthreads();
-  if (CAND) {
-    const unsigned long long c0 = cstart[blockIdx.x];
-    for (unsigned int i = threadIdx.x; i < nc; i += NT)
-      lcnt[cidx[c0 + i]] = (uint16_t) cell_count(from_key(cand[c0 + i]), slo, sntr, nb);
-    __syncthreads();
-  }
   const size_t b0 = (size_t) blockIdx.x * CH;
   int n[ROWS];
   unsigned int ex[ROWS];                       // exclusive prefix within the warp row
@@ -560,13 +542,12 @@ tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {               // all loads first
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    v[q] = (!CAND && id < N && !nt16) ? rhot[id] : (real) 0;
+    v[q] = (id < N && !nt16) ? rhot[id] : (real) 0;
   }
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    n[q] = (id >= N) ? 0 : CAND ? (int) lcnt[q * NT + threadIdx.x]
-         : (nt16 ? (int) nt16[id] : cell_count(v[q], slo, sntr, nb));
+    n[q] = (id >= N) ? 0 : (nt16 ? (int) nt16[id] : cell_count(v[q], slo, sntr, nb));
     unsigned int incl = (unsigned int) n[q];
     if (__ballot_sync(0xffffffffu, n[q] != 0)) {
 #pragma unroll
@@ -604,6 +585,64 @@ tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
     const cid_t id = (cid_t) (b0 + (size_t) q * NT + threadIdx.x);
     const unsigned long long t0 = run + pre[q * NW + w] + ex[q];
     for (int m = 0; m < n[q] && t0 + m < ntr; m++) cid[t0 + m] = id;
+  }
+}
+
+// Tracer cells from the selection's candidates only: a chunk's candidates
+// mark their places in a 4096-bit map; one thread per 32-cell word sums the
+// counts of its marked cells, a scan over the 128 words gives each word's
+// first tracer, and the thread then writes its cells' indices in cell order
+// (the same order and offsets as tracer_cell_kernel, which walks every cell
+// of the chunk).
+template <typename cid_t>
+__global__ void __launch_bounds__(NT)
+tracer_cell_cand_kernel(const BoundOut *__restrict__ bo, const unsigned long long *__restrict__ off,
+    unsigned long long ntr, cid_t *__restrict__ cid, const skey_t *__restrict__ cand,
+    const uint16_t *__restrict__ cidx, const unsigned long long *__restrict__ cstart,
+    const unsigned int *__restrict__ ccnt) {
+  constexpr int NWD = CH / 32;                  // map words
+  static_assert(NWD <= NT && NWD % 32 == 0, "one thread per map word");
+  __shared__ real slo[EZ_MAX_NT];
+  __shared__ int sntr[EZ_MAX_NT];
+  __shared__ uint16_t lcnt[CH];
+  __shared__ unsigned int bmp[NWD];
+  __shared__ unsigned int wtot[NWD / 32];
+  const unsigned int nc = ccnt[blockIdx.x];
+  if (!nc) return;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int nb = bo->nbins;
+  for (int e = t; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
+  if (t < NWD) bmp[t] = 0;
+  __syncthreads();
+  const unsigned long long c0 = cstart[blockIdx.x];
+  for (unsigned int i = t; i < nc; i += NT) {
+    const int p = cidx[c0 + i];
+    lcnt[p] = (uint16_t) cell_count(from_key(cand[c0 + i]), slo, sntr, nb);
+    atomicOr(&bmp[p >> 5], 1u << (p & 31));
+  }
+  __syncthreads();
+  unsigned int bits = 0, mine = 0;
+  if (t < NWD) {
+    bits = bmp[t];
+    for (unsigned int b = bits; b; b &= b - 1) mine += lcnt[t * 32 + __ffs(b) - 1];
+  }
+  unsigned int incl = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (t < NWD && lane == 31) wtot[w] = incl;
+  __syncthreads();
+  if (t >= NWD) return;
+  unsigned int base = 0;
+  for (int k = 0; k < w; k++) base += wtot[k];
+  unsigned long long tt = off[blockIdx.x] + base + incl - mine;
+  const size_t b0 = (size_t) blockIdx.x * CH;
+  for (unsigned int b = bits; b; b &= b - 1) {
+    const int p = t * 32 + __ffs(b) - 1;
+    const cid_t id = (cid_t) (b0 + p);
+    for (int m = 0; m < (int) lcnt[p] && tt < ntr; m++, tt++) cid[tt] = id;
   }
 }
 
@@ -1399,21 +1438,20 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   void *cidv = (N <= 0xffffffffULL) ? (void *) (cvx + iv) : (void *) cvx;
   if (N <= 0xffffffffULL) {
     if (usecand)
-      tracer_cell_kernel<uint32_t, true><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
-          (unsigned long long) nrand, (uint32_t *) cidv, nt16, cb.key, cb.idx, ps.cstart, ps.ccnt);
+      tracer_cell_cand_kernel<uint32_t><<<(unsigned) nblk, NT, 0, st>>>(bo, bscan,
+          (unsigned long long) nrand, (uint32_t *) cidv, cb.key, cb.idx, ps.cstart, ps.ccnt);
     else
-      tracer_cell_kernel<uint32_t, false><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
-          (unsigned long long) nrand, (uint32_t *) cidv, nt16, cb.key, cb.idx, ps.cstart, ps.ccnt);
+      tracer_cell_kernel<uint32_t><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
+          (unsigned long long) nrand, (uint32_t *) cidv, nt16);
   }
   else {                                            // vx and vy (iv = 0)
     if (usecand)
-      tracer_cell_kernel<unsigned long long, true><<<(unsigned) nblk, NT, 0, st>>>(rhot, N,
-          bo, bscan, (unsigned long long) nrand, (unsigned long long *) cidv, nt16, cb.key,
-          cb.idx, ps.cstart, ps.ccnt);
+      tracer_cell_cand_kernel<unsigned long long><<<(unsigned) nblk, NT, 0, st>>>(bo, bscan,
+          (unsigned long long) nrand, (unsigned long long *) cidv, cb.key, cb.idx, ps.cstart,
+          ps.ccnt);
     else
-      tracer_cell_kernel<unsigned long long, false><<<(unsigned) nblk, NT, 0, st>>>(rhot, N,
-          bo, bscan, (unsigned long long) nrand, (unsigned long long *) cidv, nt16, cb.key,
-          cb.idx, ps.cstart, ps.ccnt);
+      tracer_cell_kernel<unsigned long long><<<(unsigned) nblk, NT, 0, st>>>(rhot, N,
+          bo, bscan, (unsigned long long) nrand, (unsigned long long *) cidv, nt16);
   }
   ez_count_launch();
   if ((e = ensure_draws(m, std::max((size_t) 3 * nrand, (size_t) 1)))) return e;

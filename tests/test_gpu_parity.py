@@ -108,7 +108,7 @@ def test_dens_field_fp32_large_grids(pk_table, Ng):
     lane (512^3 is the benchmark grid), cell size of the benchmark (4.88
     Mpc/h), against the FP64 oracle within the stated FP32 field error for
     grids up to 512^3 (1e-5).  Measured: psi about 3e-7 on every grid; rho
-    1.9e-6, 4.1e-6 and 6.8e-6 on 128^3, 256^3 and 512^3, growing with the
+    1.8e-6, 3.8e-6 and 7.5e-6 on 128^3, 256^3 and 512^3, growing with the
     single-precision rounding of particle positions near the upper grid
     indices (the reference's FP32 build rounds them the same way)."""
     k, P = pk_table
