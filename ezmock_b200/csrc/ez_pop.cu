@@ -158,6 +158,8 @@ bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
   const size_t b0 = (size_t) blockIdx.x * CH;
   real r[ROWS];
   unsigned int bal[ROWS];
+  // (loads interleaved with the ballots: issuing all loads first measured
+  // slower here, 0.83 vs 0.64 ms at 512^3)
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
@@ -231,9 +233,13 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
   unsigned int bal[ROWS];
   unsigned int wc = 0;
 #pragma unroll
-  for (int q = 0; q < ROWS; q++) {
+  for (int q = 0; q < ROWS; q++) {               // all loads first
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     v[q] = (id < N) ? rhot[id] : (real) 0;
+  }
+#pragma unroll
+  for (int q = 0; q < ROWS; q++) {
+    const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     bal[q] = __ballot_sync(0xffffffffu, id < N && !(v[q] < thres));
     wc += __popc(bal[q]);
   }
