@@ -68,13 +68,6 @@ __device__ __forceinline__ T block_scan(T v, T *total, T *sw) {
   return before;
 }
 
-__device__ __forceinline__ int logb_bin(real v) {
-  // 5 - ilogb(v) clamped to [0,63]; exactly zero goes to the last bin
-  if (v == 0) return EZ_NLOGB - 1;
-  int idx = 5 - ilogb((double) v);
-  return idx < 0 ? 0 : (idx >= EZ_NLOGB ? EZ_NLOGB - 1 : idx);
-}
-
 __global__ void __launch_bounds__(NT)
 valid_count_kernel(const real *__restrict__ rho, size_t N, real thres,
     unsigned long long *cnt) {
@@ -120,39 +113,46 @@ scan_kernel(const unsigned long long *__restrict__ in, unsigned long long *out,
   if (threadIdx.x == 0) out[n] = tot;
 }
 
-// Box-Muller pairs of the bias stage (gauss_rand, pop_tracer.c:70-79): pair p
-// takes draws 2p (radius) and 2p+1 (angle) of the bias range; valid rank 2p
-// uses the cosine, 2p+1 the sine.  The multiplicative factor
-// G = 1 + g (g >= 0) or exp(g) (pop_tracer.c:288-300) is stored per rank.
-__global__ void __launch_bounds__(NT)
-gauss_pair_kernel(const uint32_t *__restrict__ draws,
-    const unsigned long long *__restrict__ nvalid, int ran, double lambda,
-    double *__restrict__ G) {
-  const size_t npair = (size_t) ((*nvalid + 1) >> 1);   // pairs for the valid cells
-  for (size_t p = (size_t) blockIdx.x * NT + threadIdx.x; p < npair;
-       p += (size_t) gridDim.x * NT) {
-    const double rr = -2 * log(ez_upos(ran, draws[2 * p]));
-    const double th = ez_u(ran, draws[2 * p + 1]) * 2 * EZ_PI;
-    const double s = lambda * sqrt(rr);
-    double sn, cs;
-    sincos(th, &sn, &cs);                     // one argument reduction for both
-    const double g0 = s * cs, g1 = s * sn;
-    G[2 * p] = (g0 >= 0) ? 1 + g0 : exp(g0);
-    G[2 * p + 1] = (g1 >= 0) ? 1 + g1 : exp(g1);
-  }
+// Bin of the log2 histogram (pop_tracer.c:264-270): 5 - ilogb(v) clamped to
+// [0, 63]; exactly zero goes to the last bin.
+#ifdef SINGLE_PREC
+// From the float's exponent field: 5 - ilogb(v) = 132 - e for a normal v;
+// zero and subnormals (e = 0) give 132, clamped to the last bin, as the
+// double-precision ilogb of their values does.
+__device__ __forceinline__ int logb_bin(float v) {
+  const int e = (int) ((__float_as_uint(v) >> 23) & 0xffu);
+  return min(max(132 - e, 0), EZ_NLOGB - 1);
 }
+#else
+__device__ __forceinline__ int logb_bin(double v) {
+  if (v == 0) return EZ_NLOGB - 1;
+  const int idx = 5 - ilogb(v);
+  return idx < 0 ? 0 : (idx >= EZ_NLOGB ? EZ_NLOGB - 1 : idx);
+}
+#endif
 
 // rho_t of the valid cells of a 4096-cell chunk (pop_tracer.c:233-300).  A
 // cell's valid rank is the chunk offset plus the valid cells before it,
-// found from per-warp ballots.
+// found from per-warp ballots.  The valid cells are then compacted in
+// shared memory (their chunk places in rank order), so the double-precision
+// Box-Muller pairs (gauss_rand, pop_tracer.c:70-79: pair p takes draws 2p
+// (radius) and 2p+1 (angle) of the bias range; rank 2p uses the cosine,
+// 2p+1 the sine) and exps run on full warps: about half of the cells are
+// valid, and a warp of mixed cells would run them for all 32 lanes.  rho_t
+// goes back to cell order through the same shared array, so the stores stay
+// coalesced.
 __global__ void __launch_bounds__(NT)
 bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
     real thres, double iexp, const unsigned long long *off,
-    const double *__restrict__ G, unsigned long long *hist) {
+    const uint32_t *__restrict__ draws, int ran, double lambda,
+    unsigned long long *hist) {
   constexpr int NW = NT / 32;
   __shared__ unsigned int pre[ROWS * NW];    // valid counts, then prefixes
   __shared__ unsigned int wsum[ROWS * NW / 32];
   __shared__ unsigned int sh[EZ_NLOGB];
+  __shared__ unsigned int snloc;             // valid cells of the chunk
+  __shared__ real st[CH];                    // clamped rho, then rho_t (cell order)
+  __shared__ uint16_t spos[CH];              // chunk place of each valid rank
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (threadIdx.x < EZ_NLOGB) sh[threadIdx.x] = 0;
   const size_t b0 = (size_t) blockIdx.x * CH;
@@ -186,29 +186,66 @@ bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
     unsigned int base = 0;
     for (int k = 0; k < w; k++) base += wsum[k];
     pre[threadIdx.x] = base + incl - c;
+    if (threadIdx.x == ROWS * NW - 1) snloc = base + incl;
   }
   __syncthreads();
-  const unsigned long long run = off[blockIdx.x];
+  // cell order: clamped rho of valid cells, 0 elsewhere; rank order: places
   const unsigned int lt = (1u << lane) - 1;
-  // all G loads first (rank order follows index order, so they coalesce)
-  double g[ROWS];
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
+    const int pos = q * NT + threadIdx.x;
     const bool valid = (bal[q] >> lane) & 1;
-    const unsigned long long rank = run + pre[q * NW + w] + __popc(bal[q] & lt);
-    g[q] = valid ? G[rank] : 0.0;
+    st[pos] = valid ? ((r[q] > (real) EZ_RHO_SAT) ? (real) EZ_RHO_SAT : r[q]) : (real) 0;
+    if (valid) spos[pre[q * NW + w] + __popc(bal[q] & lt)] = (uint16_t) pos;
   }
+  __syncthreads();
+  // one Box-Muller pair per thread and step: pair p gives ranks 2p (cos)
+  // and 2p+1 (sin); a rank outside the chunk's [run, run + nloc) belongs to
+  // the neighbouring chunk, which computes the same pair for it.  Each place
+  // is read and rewritten by the thread holding its rank only.
+  const unsigned int nloc = snloc;
+  if (nloc) {
+    const unsigned long long run = off[blockIdx.x];
+    const unsigned long long plo = run >> 1, phi = (run + nloc - 1) >> 1;
+    const unsigned int npl = (unsigned int) (phi - plo + 1);
+    for (unsigned int k0 = 0; k0 < npl; k0 += NT) {
+      const unsigned int k = k0 + threadIdx.x;
+      const bool act = k < npl;
+      const unsigned long long p = plo + k;
+      double g[2] = {0.0, 0.0};
+      if (act) {                             // gauss_rand (pop_tracer.c:70-79)
+        const double rr = -2 * log(ez_upos(ran, draws[2 * p]));
+        const double th = ez_u(ran, draws[2 * p + 1]) * 2 * EZ_PI;
+        const double s = lambda * sqrt(rr);
+        double sn, cs;
+        sincos(th, &sn, &cs);                // one argument reduction for both
+        g[0] = s * cs;
+        g[1] = s * sn;
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const unsigned long long rank = 2 * p + h;
+        const bool mine = act && rank >= run && rank < run + nloc;
+        int bin = -1;
+        if (mine) {
+          const int pos = spos[rank - run];
+          const double G = (g[h] >= 0) ? 1 + g[h] : exp(g[h]);   // pop_tracer.c:288-300
+          const real t = (1 - exp((double) st[pos] * iexp)) * G;
+          st[pos] = t;
+          bin = logb_bin(t);
+        }
+        // one shared atomic per distinct bin of the warp
+        const unsigned int grp = __match_any_sync(0xffffffffu, bin);
+        if (mine && lane == __ffs(grp) - 1) atomicAdd(&sh[bin], (unsigned int) __popc(grp));
+      }
+    }
+  }
+  __syncthreads();
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
-    if (id >= N) continue;
-    if (!((bal[q] >> lane) & 1)) { rhot[id] = 0; continue; }
-    const real v = (r[q] > (real) EZ_RHO_SAT) ? (real) EZ_RHO_SAT : r[q];
-    const real t = (1 - exp((double) v * iexp)) * g[q];
-    rhot[id] = t;
-    atomicAdd(&sh[logb_bin(t)], 1u);
+    if (id < N) rhot[id] = st[q * NT + threadIdx.x];
   }
-  __syncthreads();
   if (threadIdx.x < EZ_NLOGB && sh[threadIdx.x])
     atomicAdd(hist + threadIdx.x, (unsigned long long) sh[threadIdx.x]);
 }
@@ -1316,12 +1353,8 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   const uint32_t *dbias = nullptr;
   if ((e = ez_rng_draws(m, ran, seed, 0, nd_max, m->draws, &dbias))) return e;
   cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
-  // G per valid rank in spec[1..2] (free until the selection's sort)
-  double *G = (double *) m->spec[1];
-  gauss_pair_kernel<<<grid_for(nd_max / 2, NT), NT, 0, st>>>(dbias, bscan + nblk, ran,
-      (double) (real) EZ_GAUSS_WIDTH, G); ez_count_launch();
   bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
-      bscan, G, hist); ez_count_launch();
+      bscan, dbias, ran, (double) (real) EZ_GAUSS_WIDTH, hist); ez_count_launch();
   unsigned long long h[EZ_NLOGB], nvalid = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaMemcpyAsync(&nvalid, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
