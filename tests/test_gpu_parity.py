@@ -102,6 +102,23 @@ def test_dens_field_fp32_error(pk_table):
     assert relmax(m.field(3), rho) <= 5e-6
 
 
+@pytest.mark.parametrize("rng,fixamp,iphase,Ng,L", [
+    (0, False, False, 64, 500.0), (1, True, False, 64, 500.0), (1, False, True, 64, 500.0),
+    (0, True, True, 64, 500.0), (1, False, False, 40, 320.0), (0, True, False, 40, 320.0)])
+def test_dens_field_fp32_modes(pk_table, rng, fixamp, iphase, Ng, L):
+    """FP32 fields of both generators with fixed amplitudes and inverted
+    phases, against the FP64 oracle within the stated FP32 field error
+    (1e-5), on a grid of the warp-shuffle FFT (64^3) and of the block FFT
+    (40^3)."""
+    k, P = pk_table
+    m = make(32, Ng, L, rng, 3, k, P)
+    m.create_dens_field_from_ic(fixamp=fixamp, iphase=iphase)
+    O, t, vf, psi, rho = oracle_field(64, Ng, L, rng, 3, k, P, fixamp, iphase)
+    err = [relmax(m.field(d), psi[d]) for d in range(3)] + [relmax(m.field(3), rho)]
+    print(f"FP32 field error {Ng}^3 rng {rng} fixamp {fixamp} iphase {iphase}: {err}")
+    assert max(err) <= 1e-5
+
+
 @pytest.mark.parametrize("Ng", [128, 256, 512])
 def test_dens_field_fp32_large_grids(pk_table, Ng):
     """FP32 fields on the grids whose transforms hold 4, 8 and 16 points per
