@@ -408,13 +408,15 @@ int ez_cic(EzMesh *m, double Lbox) {
   else {
 #ifdef SINGLE_PREC
     if (Ng % OT == 0 && Ng >= 2 * OT) {
-      static bool attr = false;
       const size_t smem = 4 * OQS * sizeof(int);
-      if (!attr) {
-        cudaFuncSetAttribute(cic_owner_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-        cudaFuncSetAttribute(cic_owner_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-        attr = true;
-      }
+      // the shared-memory limit is a property of the function in each
+      // device's context: set it on every call (the instance's device is
+      // current)
+      if (!EZ_CUDA_OK(cudaFuncSetAttribute(cic_owner_kernel<2>,
+              cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)) ||
+          !EZ_CUDA_OK(cudaFuncSetAttribute(cic_owner_kernel<3>,
+              cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)))
+        return EZMOCK_ERR_UNKNOWN;
       CicStats *stats = (CicStats *) m->stats;
       unsigned int *list = m->draws;                  // free after the spectrum
       if (!m->psimax_valid) {

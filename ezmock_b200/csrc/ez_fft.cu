@@ -874,13 +874,11 @@ int ez_fft_c2r_psi(EzMesh *m) {
   int R = 4;
   while (R > 1 && sizeof(cplx) * (2 * (size_t) Nh + 3 * R * (Nh + 1) + 2 * (size_t) Nh * 3 * R) > 160 * 1024) R >>= 1;
   const size_t sm_k = sizeof(cplx) * (2 * (size_t) Nh + 3 * R * (size_t) (Nh + 1) + 2 * (size_t) Nh * 3 * R);
-  static int attr_done = 0;
-  if (!attr_done) {
-    cudaFuncSetAttribute(fft_pass_i, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(fft_pass_j, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(fft_pass_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done = 1;
-  }
+  // per-device function attributes: set on every call (current device)
+  if (!EZ_CUDA_OK(cudaFuncSetAttribute(fft_pass_i, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) ||
+      !EZ_CUDA_OK(cudaFuncSetAttribute(fft_pass_j, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) ||
+      !EZ_CUDA_OK(cudaFuncSetAttribute(fft_pass_k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)))
+    return EZMOCK_ERR_UNKNOWN;
   const int nkt = (m->Nk + K - 1) / K;
   ez_stage_begin(m, ST_FFT_I);
   fft_pass_i<<<dim3(Ng, nkt), FFT_NT, sm_i, m->stream>>>(m->spec[0], m->spec[1],
@@ -922,12 +920,9 @@ int ez_fft_r2c(int dev, cudaStream_t st, const real *in, cplx *out, int Ng, int 
   const size_t sm_r = sizeof(cplx) * (2 * (size_t) Nh + 1 + 2 * (size_t) Nh * R);
   const int K = ez_fft_tile_k(Ng);
   const size_t sm_a = sizeof(cplx) * ((size_t) Ng + 2 * (size_t) Ng * K);
-  static int attr_done = 0;
-  if (!attr_done) {
-    cudaFuncSetAttribute(fft_r2c_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(fft_axis_one<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done = 1;
-  }
+  if (!EZ_CUDA_OK(cudaFuncSetAttribute(fft_r2c_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) ||
+      !EZ_CUDA_OK(cudaFuncSetAttribute(fft_axis_one<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)))
+    return EZMOCK_ERR_UNKNOWN;
   const size_t nrows = (size_t) Ng * Ng;
   fft_r2c_rows<<<(unsigned) ((nrows + R - 1) / R), FFT_NT, sm_r, st>>>(
       in, out, Ng, Nkp, R, nrows, ph, twg); ez_count_launch();

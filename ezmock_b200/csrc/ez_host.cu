@@ -592,7 +592,12 @@ int EZmock_create_dens_field(EZMOCK *ez, real *psi[3], bool deepcopy,
   }
   if (user_psi || delta) side_streams(ez);
   if ((e = ez_cic(m, conf->Lbox))) return (*err = e);
-  if (!EZ_CUDA_OK(cudaStreamSynchronize(m->stream))) return (*err = EZMOCK_ERR_UNKNOWN);
+  // A field made from the initial conditions returns with its kernels still
+  // queued: every later call of the instance is ordered after them on the
+  // instance stream.  With caller arrays (psi, delta) the call waits, since
+  // a copy from page-locked host memory may still be reading them.
+  if ((user_psi || delta) && !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
+    return (*err = EZMOCK_ERR_UNKNOWN);
   m->fixamp = fixamp;
   m->iphase = iphase;
   m->have_field = true;

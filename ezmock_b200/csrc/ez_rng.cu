@@ -148,12 +148,16 @@ uint64_t splitmix64(uint64_t *z) {
 }
 
 std::mutex g_mrg_mu;
-int g_mrg_dev_ready = -1;                 // device id whose tables are set
-uint32_t *g_mrg_thread_jump = nullptr;    // device, MRG_THREADS x 18
+// per device (constant-memory tables and a global copy of the thread jumps
+// live in each device's context): tables set, thread jumps
+constexpr int EZ_MAX_DEV = 64;
+bool g_mrg_dev_ready[EZ_MAX_DEV];
+uint32_t *g_mrg_thread_jump[EZ_MAX_DEV];  // device, MRG_THREADS x 18
 
 int mrg_prepare(int dev) {
   std::lock_guard<std::mutex> lk(g_mrg_mu);
-  if (g_mrg_dev_ready == dev) return 0;
+  if (dev < 0 || dev >= EZ_MAX_DEV) return EZMOCK_ERR_UNKNOWN;
+  if (g_mrg_dev_ready[dev]) return 0;
   uint64_t p1[64][9], p2[64][9];
   const uint64_t a1[9] = {0, 1, 0, 0, 0, 1, M1 - A13N, A12, 0};
   const uint64_t a2[9] = {0, 1, 0, 0, 0, 1, M2 - A23N, 0, A21};
@@ -182,12 +186,14 @@ int mrg_prepare(int dev) {
     hmat_mul(s1, g1, g1, M1);
     hmat_mul(s2, g2, g2, M2);
   }
-  if (g_mrg_thread_jump) cudaFree(g_mrg_thread_jump);
-  if (!EZ_CUDA_OK(cudaMalloc(&g_mrg_thread_jump, tj.size() * 4)) ||
-      !EZ_CUDA_OK(cudaMemcpy(g_mrg_thread_jump, tj.data(), tj.size() * 4,
-          cudaMemcpyHostToDevice)))
+  uint32_t *&tjd = g_mrg_thread_jump[dev];
+  if (!tjd && !EZ_CUDA_OK(cudaMalloc(&tjd, tj.size() * 4))) {
+    tjd = nullptr;
     return EZMOCK_ERR_MEMORY;
-  g_mrg_dev_ready = dev;
+  }
+  if (!EZ_CUDA_OK(cudaMemcpy(tjd, tj.data(), tj.size() * 4, cudaMemcpyHostToDevice)))
+    return EZMOCK_ERR_MEMORY;
+  g_mrg_dev_ready[dev] = true;
   return 0;
 }
 
@@ -204,7 +210,7 @@ int mrg_fill_st(int dev, cudaStream_t st, uint64_t seed, uint64_t start,
   if (!nblk) return 0;
   mrg_fill_kernel<<<(unsigned) nblk, MRG_THREADS, 0, st>>>(
       (uint32_t) s1[0], (uint32_t) s1[1], (uint32_t) s1[2], (uint32_t) s2[0],
-      (uint32_t) s2[1], (uint32_t) s2[2], start, count, g_mrg_thread_jump, out); ez_count_launch();
+      (uint32_t) s2[1], (uint32_t) s2[2], start, count, g_mrg_thread_jump[dev], out); ez_count_launch();
   return EZ_CUDA_OK(cudaGetLastError()) ? 0 : EZMOCK_ERR_UNKNOWN;
 }
 
@@ -661,18 +667,23 @@ void build_mt_tables(MtTables &T) {
 std::mutex g_mt_mu;
 MtTables g_mt;
 bool g_mt_built = false;
-int g_mt_dev_ready = -1;
-int g_mt_nsm = 148;                          // SMs of the prepared device
-uint64_t *g_mt_xpow_dev = nullptr;
+// per device: set up, SM count, device copy of the x^(2^k) table
+bool g_mt_dev_ready[EZ_MAX_DEV];
+int g_mt_nsm[EZ_MAX_DEV];
+uint64_t *g_mt_xpow_dev[EZ_MAX_DEV];
 
 int mt_prepare(int dev) {
   std::lock_guard<std::mutex> lk(g_mt_mu);
   if (!g_mt_built) { build_mt_tables(g_mt); g_mt_built = true; }
   if (!g_mt.ok) return EZMOCK_ERR_RNG_SET;
-  if (g_mt_dev_ready == dev) return 0;
-  if (g_mt_xpow_dev) cudaFree(g_mt_xpow_dev);
-  if (!EZ_CUDA_OK(cudaMalloc(&g_mt_xpow_dev, g_mt.xpow.size() * 8)) ||
-      !EZ_CUDA_OK(cudaMemcpy(g_mt_xpow_dev, g_mt.xpow.data(), g_mt.xpow.size() * 8,
+  if (dev < 0 || dev >= EZ_MAX_DEV) return EZMOCK_ERR_UNKNOWN;
+  if (g_mt_dev_ready[dev]) return 0;
+  uint64_t *&xp = g_mt_xpow_dev[dev];
+  if (!xp && !EZ_CUDA_OK(cudaMalloc(&xp, g_mt.xpow.size() * 8))) {
+    xp = nullptr;
+    return EZMOCK_ERR_MEMORY;
+  }
+  if (!EZ_CUDA_OK(cudaMemcpy(xp, g_mt.xpow.data(), g_mt.xpow.size() * 8,
           cudaMemcpyHostToDevice)))
     return EZMOCK_ERR_MEMORY;
   if (!EZ_CUDA_OK(cudaFuncSetAttribute(mt_horner_kernel,
@@ -682,9 +693,9 @@ int mt_prepare(int dev) {
           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (JD_XL * sizeof(uint32_t)))) ||
       !EZ_CUDA_OK(cudaFuncSetAttribute(mt_jumpd_kernel,
           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) JD_SMEM)) ||
-      !EZ_CUDA_OK(cudaDeviceGetAttribute(&g_mt_nsm, cudaDevAttrMultiProcessorCount, dev)))
+      !EZ_CUDA_OK(cudaDeviceGetAttribute(&g_mt_nsm[dev], cudaDevAttrMultiProcessorCount, dev)))
     return EZMOCK_ERR_UNKNOWN;
-  g_mt_dev_ready = dev;
+  g_mt_dev_ready[dev] = true;
   return 0;
 }
 
@@ -778,7 +789,7 @@ int mt_prepare_ranges(EzMesh *m, uint64_t seed, MtRange *r, int nr,
   for (int lev = 0; lev <= pmax; lev++) {
     if (!lev_n[lev]) continue;
     mt_horner_kernel<<<lev_n[lev], H_THREADS, smem, m->stream>>>(states,
-        d_desc + lev_off[lev], g_mt_xpow_dev, d_plist); ez_count_launch();
+        d_desc + lev_off[lev], g_mt_xpow_dev[m->device], d_plist); ez_count_launch();
   }
   // (copies from pageable host memory are staged before cudaMemcpyAsync
   // returns, so the host vectors may be released here)
@@ -905,7 +916,7 @@ int mt_jump_launch(int dev, cudaStream_t st, uint32_t *states, uint64_t seed,
   // the stream words after the states; two blocks per SM in one wave
   uint32_t *xs = states + (base + nst) * MT_N;
   const int ncg = (int) ((nst + 31) / 32);
-  const int nseg = std::max(1, std::min(JD_N8, 2 * g_mt_nsm / ncg));
+  const int nseg = std::max(1, std::min(JD_N8, 2 * g_mt_nsm[dev] / ncg));
   if (!EZ_CUDA_OK(cudaMemsetAsync(states + base * MT_N, 0, nst * MT_N * sizeof(uint32_t), st)))
     return EZMOCK_ERR_UNKNOWN;
   mt_seq_kernel<<<1, JD_SEQ_THREADS, JD_XL * sizeof(uint32_t), st>>>(a, xs);

@@ -252,6 +252,9 @@ class RefLib:
         L.EZmock_destroy.argtypes = [_vp]
         L.EZmock_errmsg.restype = ctypes.c_char_p
         L.EZmock_errmsg.argtypes = [ctypes.c_int]
+        L.EZmock_write_ascii.restype = ctypes.c_int
+        L.EZmock_write_ascii.argtypes = [_vp] + [_vp] * 6 + [ctypes.c_size_t, ctypes.c_double,
+                                                             ctypes.c_bool, ctypes.c_char_p, ip]
         L.ezref_mesh_ptr.restype = _vp
         L.ezref_mesh_ptr.argtypes = [_vp, ctypes.c_int]
         L.ezref_growth2.restype = ctypes.c_double
@@ -343,6 +346,16 @@ class _RefMock:
                                      ctypes.byref(self.err))
         self._chk()
         return nt.reshape((self.Ng,) * 3), pdf_out, nc.value, no.value
+
+    def write_ascii(self, cat, fname, rsd_fac=0.0, header=True):
+        """The reference's EZmock_write_ascii (save_res.c:95-178) on six
+        arrays; returns its error code."""
+        arrs = [np.ascontiguousarray(a, self.o.rdt) for a in cat]
+        err = ctypes.c_int(0)
+        self.o.lib.EZmock_write_ascii(self.ez, *[_ptr(a) for a in arrs], len(arrs[0]),
+                                      float(rsd_fac), bool(header), str(fname).encode(),
+                                      ctypes.byref(err))
+        return err.value
 
     def populate(self, params, nexp, att_part=False):
         prm = np.array(params, self.o.rdt)

@@ -1,9 +1,10 @@
 """EZmockB200_mt19937_fill_noalloc: the MT19937 fill with static device scratch.
 
 It must give the same draws as the allocating entry point EZmockB200_rng_raw
-(randgen 1), call after call, and reject requests larger than its scratch
-before touching the GPU.  This file is named to be collected last, so the GPU
-test also runs after every other test has used the library in the process.
+(randgen 1) and as the CPU oracle's MT19937 stream, call after call, and
+reject requests larger than its scratch before touching the GPU.  This file
+is named to be collected last, so the GPU test also runs after every other
+test has used the library in the process.
 """
 import ctypes
 
@@ -11,6 +12,7 @@ import numpy as np
 import pytest
 
 from ezmock_b200 import _lib
+from oracle.pyoracle import Oracle
 
 MAX_DRAWS = 1 << 47
 ERR_SCRATCH_SIZE = 64
@@ -52,9 +54,12 @@ def test_noalloc_matches_allocating_fill():
                                               ctypes.c_void_p(stream.cuda_stream))
         assert e == 0, L.EZmock_errmsg(e).decode()
     torch.cuda.synchronize()
+    O = Oracle(64)
     for (seed, start, n), b in zip(cases, bufs):
         got = b.cpu().numpy().view(np.uint32)
         np.testing.assert_array_equal(got, _rng_raw(L, seed, start, n))
+        # independently of the library's jump tables and generation kernels
+        np.testing.assert_array_equal(got, O.rng_raw(1, seed, start, n))
     # again, on the legacy default stream, into the first buffer
     seed, start, n = cases[1]
     b = bufs[1]
