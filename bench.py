@@ -37,6 +37,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from ezmock_b200.replicas import job_seconds_per_mock  # noqa: E402
+
 METRIC = "s/mock at 512^3 (FP32 production mode)"
 STAGES = ["rng", "ic", "fft_i", "fft_j", "fft_k", "cic", "bias", "select", "emit", "vel",
           "d2h"]
@@ -206,12 +208,17 @@ class ClockSampler:
                 "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
-def cpu_reference(cfg, k, P, steps, warmup, allow_scale=True):
+def cpu_reference(cfg, k, P, steps, warmup, allow_scale=True, budget_s=240.0):
     """The reference's libEZmock (oracle/_ref, OpenMP, all host threads) on the
-    workload; returns (s/mock, sample description, threads)."""
+    workload.  Returns a dict: s/mock (median), its create_dens_field and
+    populate_tracer parts (medians), the wall time of the three c2r FFTs of
+    one field through the same FFTW interface (the project CPU FFT, FFTW3
+    being absent), the sample description and the thread count."""
     from oracle.pyoracle import RefLib
     R = RefLib(32, nthread=0)
     nthreads = os.cpu_count()
+    R.lib.ezref_fft_c2r_seconds.restype = ctypes.c_double
+    R.lib.ezref_fft_c2r_seconds.argtypes = [ctypes.c_int, ctypes.c_int]
 
     def one(Ng, Lbox, seed):
         m = R.new(Lbox, Ng, cfg.rng, seed)
@@ -219,132 +226,109 @@ def cpu_reference(cfg, k, P, steps, warmup, allow_scale=True):
         m.setup_pk(k, P)
         t0 = time.perf_counter()
         m.create()
+        t1 = time.perf_counter()
         for n_t, *par in cfg.population_list():
             m.populate(par, int(round(n_t * Lbox ** 3)))
-        return time.perf_counter() - t0
+        t2 = time.perf_counter()
+        return t2 - t0, t1 - t0, t2 - t1
 
-    # a 256^3 probe decides whether full-size steps fit in a few minutes
-    ng_s = cfg.Ng // 2
-    t_small = one(ng_s, cfg.Lbox / 2, 1)
-    est = t_small * 8 * math.log(cfg.Ng ** 3) / math.log(ng_s ** 3)
-    if est * (steps + min(warmup, 1)) < 240 or not allow_scale:
+    def run(Ng, Lbox, scale, what):
         for w in range(min(warmup, 1)):
-            one(cfg.Ng, cfg.Lbox, 1000 + w)
-        ts = [one(cfg.Ng, cfg.Lbox, 1 + s) for s in range(steps)]
-        return (statistics.median(ts), f"{steps} full {cfg.Ng}^3 mocks (median), "
-                f"{nthreads} OpenMP threads", nthreads)
-    ts = [one(ng_s, cfg.Lbox / 2, 1 + s) for s in range(steps)]
+            one(Ng, Lbox, 1000 + w)
+        ts = [one(Ng, Lbox, 1 + s) for s in range(steps)]
+        med = [statistics.median(t[i] for t in ts) * scale for i in range(3)]
+        fft = R.lib.ezref_fft_c2r_seconds(Ng, 0) * scale
+        return {"value": med[0], "create_s": med[1], "populate_s": med[2], "fft_s": fft,
+                "sample": f"{what}, {nthreads} OpenMP threads; 1 warm-up, median of {steps}; "
+                          "FFT: project CPU FFT (FFTW3 not installed), "
+                          f"3 c2r FFTs {fft:.2f} s of the create_dens_field part",
+                "cores": nthreads}
+
+    # a half-size probe decides whether full-size steps fit in the budget
+    ng_s = cfg.Ng // 2
     scale = 8 * math.log(cfg.Ng ** 3) / math.log(ng_s ** 3)
-    return (statistics.median(ts) * scale,
-            f"{steps} mocks at {ng_s}^3 (median) x {scale:.2f} (N log N scaling to "
-            f"{cfg.Ng}^3), {nthreads} OpenMP threads", nthreads)
+    t_small = one(ng_s, cfg.Lbox / 2, 1)[0]
+    if t_small * scale * (steps + min(warmup, 1)) < budget_s or not allow_scale:
+        return run(cfg.Ng, cfg.Lbox, 1.0, f"{steps} full {cfg.Ng}^3 mocks")
+    return run(ng_s, cfg.Lbox / 2, scale,
+               f"{steps} mocks at {ng_s}^3, box {cfg.Lbox / 2:g} (the same cell size and "
+               f"tracer densities) x {scale:.2f} (N log N scaling to {cfg.Ng}^3)")
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="single512")
-    ap.add_argument("--rng", type=int, default=None, help="0 MRG32k3a, 1 MT19937")
-    ap.add_argument("--prec", type=int, default=32)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    args = ap.parse_args()
+def config_of(cfg, n_gpus, b):
+    """The workload description both arms print (identical dicts)."""
+    pops = [int(round(n_t * cfg.Lbox ** 3)) for n_t, *_ in cfg.population_list()]
+    return {"workload": workload_desc(cfg), "Ngrid": cfg.Ng, "Lbox": cfg.Lbox,
+            "nexp": pops[0] if len(pops) == 1 else pops,
+            "parallelism": f"replicas x{n_gpus}",
+            "l2": f"inputs larger than L2 (psi {3 * cfg.Ng ** 3 * b / 1e9:.1f} GB, "
+                  f"spectra {3 * cfg.Ng ** 2 * (cfg.Ng // 2 + 1) * 2 * b / 1e9:.1f} GB per mock)"}
 
-    from ezmock_b200.workloads import CONFIGS, bbks_pk
-    cfg = CONFIGS[args.workload]
-    if args.rng is not None:
-        cfg.rng = args.rng
-    k, P = bbks_pk()
-    from ezmock_b200.replicas import Replicas, job_seconds_per_mock, rank_env, rank_seed
-    rank, world, local = rank_env()
-    n_gpus = max(world, 1)
 
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        try:
-            v, sample, cores = cpu_reference(cfg, k, P, args.steps, args.warmup)
-        except Exception as e:             # the reference build is missing
-            print(json.dumps({"impl": "reference", "unavailable": f"reference build: {e}"}))
-            return 0
-        print(json.dumps({
-            "impl": "reference", "metric": METRIC, "value": v, "unit": "s/mock",
-            "n_gpus": n_gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic BBKS P(k)",
-            "config": {"workload": workload_desc(cfg), "Ngrid": cfg.Ng, "Lbox": cfg.Lbox},
-            "cpu_baseline": {"value": v, "unit": "s/mock", "cores": cores, "kind": "reference",
-                             "sample": sample + "; FFT: project CPU FFT (FFTW3 not installed)"},
-            "e2e": {"value": v, "unit": "s/mock", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}))
-        return 0
+def survey_bytes(cfg, b, ntr):
+    """Compulsory HBM bytes of one whole mock (three c2r FFTs as two sweeps
+    each with the spectrum generated on-chip, CIC, bias/select and emission
+    per population, velocity painting, catalogue)."""
+    N = cfg.Ng ** 3
+    H = cfg.Ng ** 2 * (cfg.Ng // 2 + 1) * 2 * b
+    npop = len(cfg.population_list())
+    return 3 * (2 * H + N * b) + 4 * N * b + npop * (4 * N * b + 2 * N + 4 * N) + 6 * N * b + 6 * b * ntr
 
-    if world > 1:
-        import torch
-        torch.cuda.set_device(local)
-    rep = Replicas(world, "nccl")
 
-    from ezmock_b200 import EZmock
-    m = EZmock(Lbox=cfg.Lbox, Ngrid=cfg.Ng, rng=cfg.rng, seed=rank_seed(rank),
-               prec=args.prec)
-    L = m._L
-    m.set_option(3, local)            # device
-    m.set_option(2, 1)                # stage timings
-    m.eval_growth_params(cfg.z, cfg.omega_m)
-    m.setup_linear_pk(k, P)
-    # one or more populations of the same field: (nexp, [rho_c, rho_exp, pdf_base, sigma_v])
+def measure(cfg, args, m, L, k, P, rep, local, n_gpus, seed0, clk):
+    """Device-timed steps, a stage-timing pass and end-to-end steps of one
+    workload on instance m; returns the line's measured keys."""
     pops = [(int(round(n_t * cfg.Lbox ** 3)), par) for n_t, *par in cfg.population_list()]
     b = 4 if args.prec == 32 else 8
+    seed = [seed0]
 
-    def barrier():
-        rep.barrier()
-
-    def reduce_max(x):
-        return rep.reduce_max(x, f"cuda:{local}")
-
-    seed = [rank_seed(rank)]
-
-    def device_step():
+    def device_step(timing):
         seed[0] += 1
         m.set_option(4, seed[0])
         m.create_dens_field_from_ic()
-        stage_c = m.stage_times()
+        stage_c = m.stage_times() if timing else {}
         n, stage_p = 0, {}
         for nexp_i, par in pops:
             n += m.populate_device(*par, nexp_i)
-            for s_, v_ in m.stage_times().items():
-                if v_ >= 0:
-                    stage_p[s_] = stage_p.get(s_, 0.0) + v_
+            if timing:
+                for s_, v_ in m.stage_times().items():
+                    if v_ >= 0:
+                        stage_p[s_] = stage_p.get(s_, 0.0) + v_
         return n, stage_c, stage_p
 
-    clk = ClockSampler(local)
-    clk.start()
+    m.set_option(2, 0)                       # no per-stage events in the timed region
     for _ in range(args.warmup):
-        device_step()
+        device_step(False)
     m.sync()
-    barrier()
+    rep.barrier()
     l0 = L.EZmockB200_launch_count()
     L.EZmockB200_mark(m._ez, 0)
     t0 = time.perf_counter()
-    stage_acc = {s: [] for s in STAGES}
     ntr = 0
     for _ in range(args.steps):
-        ntr, st_c, st_p = device_step()
-        for s in STAGES:
-            v = st_p.get(s, -1) if s not in ("rng", "ic", "fft_i", "fft_j", "fft_k", "cic") else st_c[s]
-            if v >= 0:
-                stage_acc[s].append(v)
+        ntr = device_step(False)[0]
     L.EZmockB200_mark(m._ez, 1)
     ms = ctypes.c_double()
     L.EZmockB200_elapsed(m._ez, 0, 1, ctypes.byref(ms))
     wall = time.perf_counter() - t0
     launches = L.EZmockB200_launch_count() - l0
-    clk.mark(t0, t0 + wall)
-    barrier()
-    t_dev = reduce_max(ms.value / 1e3)
+    if clk is not None:
+        clk.mark(t0, t0 + wall)
+    rep.barrier()
+    t_dev = rep.reduce_max(ms.value / 1e3, f"cuda:{local}")
     value = job_seconds_per_mock(t_dev, n_gpus, args.steps)
+
+    # stage times: a separate pass with CUDA events around every stage
+    m.set_option(2, 1)
+    stage_acc = {s: [] for s in STAGES}
+    for _ in range(min(args.steps, 5)):
+        _, st_c, st_p = device_step(True)
+        for s in STAGES:
+            v = st_c.get(s, -1) if s in ("rng", "ic", "fft_i", "fft_j", "fft_k", "cic") \
+                else st_p.get(s, -1)
+            if v >= 0:
+                stage_acc[s].append(v)
+    m.set_option(2, 0)
 
     # end to end through the public API with host buffers
     def e2e_step():
@@ -358,12 +342,10 @@ def main():
             n += len(cat[0])
         return n
 
-    # untimed warm-up of the host path (the catalogue's host blocks are
-    # prepared after each copy-out; the device steps above used none)
     for _ in range(args.warmup):
         e2e_step()
     m.sync()
-    barrier()
+    rep.barrier()
     L.EZmockB200_mark(m._ez, 2)
     te0 = time.perf_counter()
     n_out = 0
@@ -373,50 +355,136 @@ def main():
     e2e_wall = time.perf_counter() - te0
     ems = ctypes.c_double()
     L.EZmockB200_elapsed(m._ez, 2, 3, ctypes.byref(ems))
-    e2e = job_seconds_per_mock(reduce_max(max(ems.value / 1e3, e2e_wall)), n_gpus, args.steps)
-    # the sampler stops after every timed region
-    clocks = clk.stop()
+    e2e = job_seconds_per_mock(rep.reduce_max(max(ems.value / 1e3, e2e_wall), f"cuda:{local}"),
+                               n_gpus, args.steps)
     h2d = 3 * pk_trim_len(k, cfg.Ng, cfg.Lbox) * 8
     d2h = 6 * n_out * b
 
-    # roofline of the dominant kernel
     peak, peak_kind = read_peak()
     algo = algorithmic_bytes(cfg.Ng, b)
     med = {s: statistics.median(v) for s, v in stage_acc.items() if v}
-    stages_gbs = {s: {"ms": round(med[s], 4),
-                      "GB/s": round(algo[s] / (med[s] * 1e-3) / 1e9, 1) if s in algo else None}
-                  for s in med}
+    stages = {s: {"ms": round(med[s], 4),
+                  "GB/s": round(algo[s] / (med[s] * 1e-3) / 1e9, 1) if s in algo else None}
+              for s in med}
     dom = max((s for s in algo if s in med), key=lambda s: med[s])
     achieved = algo[dom] / (med[dom] * 1e-3) / 1e9
     traffic = read_traffic(cfg.name).get(dom)
     roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "algorithmic_bytes": algo[dom]}
+    whole = survey_bytes(cfg, b, ntr)
+    mock_roof = {"bytes": whole, "achieved_GBs": round(whole / value / 1e9, 1),
+                 "frac": round(whole / value / 1e9 / peak, 4)}
+    return {"value": value, "ms_per_step": t_dev * 1e3 / args.steps, "ntracer": ntr,
+            "e2e": {"value": e2e, "unit": "s/mock", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "roofline": roof, "mock_roofline": mock_roof,
+            "stages": stages, "wall_s_per_mock": wall / args.steps}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="single512")
+    ap.add_argument("--rng", type=int, default=None, help="0 MRG32k3a, 1 MT19937")
+    ap.add_argument("--prec", type=int, default=32)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-multi1024", action="store_true",
+                    help="skip the 1024^3 three-population sub-measurement")
+    args = ap.parse_args()
+
+    from ezmock_b200.workloads import CONFIGS, bbks_pk
+    cfg = CONFIGS[args.workload]
+    if args.rng is not None:
+        cfg.rng = args.rng
+    k, P = bbks_pk()
+    from ezmock_b200.replicas import Replicas, rank_env, rank_seed
+    rank, world, local = rank_env()
+    n_gpus = max(world, 1)
+    b = 4 if args.prec == 32 else 8
+    config = config_of(cfg, n_gpus, b)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        try:
+            cb = cpu_reference(cfg, k, P, args.steps, args.warmup)
+        except Exception as e:             # the reference build is missing
+            print(json.dumps({"impl": "reference", "unavailable": f"reference build: {e}"}))
+            return 0
+        v = cb["value"]
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "s/mock",
+            "n_gpus": n_gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.prec == 32 else "f64",
+            "data": "synthetic (BBKS P(k), sigma_8 = 0.81)", "config": config,
+            "cpu_baseline": dict(cb, unit="s/mock", kind="reference"),
+            "e2e": {"value": v, "unit": "s/mock", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return 0
+
+    if world > 1:
+        import torch
+        torch.cuda.set_device(local)
+    rep = Replicas(world, "nccl")
+
+    from ezmock_b200 import EZmock
+    m = EZmock(Lbox=cfg.Lbox, Ngrid=cfg.Ng, rng=cfg.rng, seed=rank_seed(rank), prec=args.prec)
+    L = m._L
+    m.set_option(3, local)            # device
+    m.eval_growth_params(cfg.z, cfg.omega_m)
+    m.setup_linear_pk(k, P)
+    clk = ClockSampler(local)
+    clk.start()
+    res = measure(cfg, args, m, L, k, P, rep, local, n_gpus, rank_seed(rank), clk)
+    del m
+
+    sub = None
+    if args.workload == "single512" and not args.no_multi1024 and args.prec == 32:
+        # the 1024^3 mock with three populations of one field, measured the
+        # same way (fewer steps), as a sub-object of the same line
+        c2 = CONFIGS["multi1024"]
+        a2 = argparse.Namespace(**vars(args))
+        a2.steps, a2.warmup = min(args.steps, 5), min(args.warmup, 3)
+        m2 = EZmock(Lbox=c2.Lbox, Ngrid=c2.Ng, rng=c2.rng, seed=rank_seed(rank) + 7919,
+                    prec=args.prec)
+        m2.set_option(3, local)
+        m2.eval_growth_params(c2.z, c2.omega_m)
+        m2.setup_linear_pk(k, P)
+        r2 = measure(c2, a2, m2, m2._L, k, P, rep, local, n_gpus, rank_seed(rank) + 7919, None)
+        del m2
+        sub = dict(r2, metric="s/mock at 1024^3 (FP32, three populations of one field)",
+                   unit="s/mock", steps=a2.steps, warmup=a2.warmup,
+                   config=config_of(c2, n_gpus, b))
+        if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
+            try:
+                cb2 = cpu_reference(c2, k, P, 3, 1, budget_s=30.0)
+                sub["cpu_baseline"] = dict(cb2, unit="s/mock", kind="reference")
+            except Exception as e:
+                sub["cpu_baseline"] = {"value": None, "sample": f"unavailable: {e}"}
+    # the sampler stops after every timed region
+    clocks = clk.stop()
 
     line = {
-        "metric": METRIC, "value": value, "unit": "s/mock", "n_gpus": n_gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev * 1e3 / args.steps,
+        "metric": METRIC, "value": res["value"], "unit": "s/mock", "n_gpus": n_gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.prec == 32 else "f64",
-        "data": "synthetic (BBKS P(k), sigma_8 = 0.81)",
-        "config": {"workload": workload_desc(cfg), "Ngrid": cfg.Ng, "Lbox": cfg.Lbox,
-                   "nexp": pops[0][0] if len(pops) == 1 else [p_[0] for p_ in pops],
-                   "ntracer": ntr, "parallelism": f"replicas x{n_gpus}",
-                   "l2": f"inputs larger than L2 (psi {3 * cfg.Ng ** 3 * b / 1e9:.1f} GB, "
-                         f"spectra {3 * cfg.Ng ** 2 * (cfg.Ng // 2 + 1) * 2 * b / 1e9:.1f} GB "
-                         "per mock)"},
-        "e2e": {"value": e2e, "unit": "s/mock", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches, "roofline": roof, "stages": stages_gbs,
-        "clocks": clocks, "wall_s_per_mock": wall / args.steps,
+        "data": "synthetic (BBKS P(k), sigma_8 = 0.81)", "config": config,
+        "ntracer": res["ntracer"], "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
+        "roofline": res["roofline"], "mock_roofline": res["mock_roofline"],
+        "stages": res["stages"], "clocks": clocks, "wall_s_per_mock": res["wall_s_per_mock"],
     }
+    if sub is not None:
+        line["multi1024"] = sub
     if rank == 0 and n_gpus == 1 and not args.no_cpu_baseline:
         try:
-            v, sample, cores = cpu_reference(cfg, k, P, 1, 0)
-            line["cpu_baseline"] = {"value": v, "unit": "s/mock", "cores": cores,
-                                    "kind": "reference",
-                                    "sample": sample + "; FFT: project CPU FFT "
-                                    "(FFTW3 not installed)"}
+            cb = cpu_reference(cfg, k, P, 3, 1, budget_s=60.0)
+            line["cpu_baseline"] = dict(cb, unit="s/mock", kind="reference")
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unit": "s/mock", "cores": None,
                                     "kind": "reference", "sample": f"unavailable: {e}"}

@@ -294,6 +294,205 @@ cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
   }
 }
 
+// ---- owner-computes kernel on 32 x 32 column tiles (FP32, Ng % 32 == 0) ----
+//
+// A CTA owns a 32 x 32 column of cells over a z range [zs, ze) (the grid is
+// cut along z as well, so that the CTAs fill whole waves of one CTA per SM)
+// and walks it in chunks of CZ = 4 slices.  Each of its 768 threads owns two
+// of the (32 + 2 OH + 1)^2 Lagrangian columns whose particles can reach the
+// tile, for the whole walk: its column's coordinates, wrapped lattice
+// indices and output offsets are computed once, and a chunk's four particles
+// of a column arrive as one 16-byte load per displacement field, issued one
+// column ahead.  Accumulation is 32-bit fixed point in a shared-memory ring
+// of three chunks laid out [quantity][slot][x][y] with y fastest: the lanes
+// of a warp hold consecutive Lagrangian columns along y, so a deposit's bank
+// is its y cell, and lanes collide only where the flow compresses along y
+// (distinct cells in one bank or the same cell).  Chunk c's particles reach
+// chunks c-1 .. c+1; chunk c-1 is final after chunk c and is written with
+// plain 16-byte stores (its four slices of one cell row and quantity).
+// Particles displaced by more than OH cells are listed by the CTA that owns
+// their Lagrangian cell and deposited by fixup_kernel, as in the kernel
+// above; the fixed-point scales and the overflow bound are the same.
+constexpr int TT = 32;                        // tile side (x and y)
+constexpr int CZ = 4;                         // z slices per chunk
+constexpr int TRS = 3 * CZ;                   // ring slots
+constexpr int TNT = 768;                      // threads: two columns each
+constexpr int TQS = TRS * TT * TT;            // ints per quantity
+constexpr int TSLOT = TT * TT;                // ints per slot
+
+template <int OH>
+__global__ void __launch_bounds__(TNT, 1)
+cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
+    const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
+    int Ng, real igs, CicStats *stats, unsigned int *list, int nzs) {
+  constexpr int OW = TT + 2 * OH + 1;         // Lagrangian columns per side
+  constexpr int OB = OH + 1;                  // read origin: i0 - OB, j0 - OB
+  constexpr int NCOL = OW * OW;
+  static_assert(NCOL <= 2 * TNT, "two columns per thread");
+  extern __shared__ __align__(16) int tring[];  // [4][TRS][TT][TT]
+  const int ntile = Ng / TT;
+  const int tile = blockIdx.x / nzs, zsp = blockIdx.x - tile * nzs;
+  const int i0 = (tile / ntile) * TT, j0 = (tile % ntile) * TT;
+  const int zlen = Ng / nzs;
+  const int zs = zsp * zlen, ze = zs + zlen;
+  const int cfirst = zs / CZ - 1, clast = ze / CZ;
+  const float pmax = fmaxf(__uint_as_float(stats->psimax_bits), 1e-30f);
+  const float mscale = exp2f(floorf(log2f(2147483647.f / (1024.f * pmax))));
+  const float minv = 1.f / mscale;
+  for (int e = threadIdx.x; e < TQS; e += TNT)      // 4 * TQS ints as int4
+    reinterpret_cast<int4 *>(tring)[e] = make_int4(0, 0, 0, 0);
+
+  // the thread's two columns (the second may be past the last one)
+  struct Col {
+    int cxo, cyo;          // tile coordinates of the Lagrangian column
+    int iw, jw;            // wrapped lattice indices
+    float iwf, jwf;
+    size_t base;           // offset of the column's z = 0 particle
+    bool own, valid;
+  };
+  auto setup = [&](int col, Col &C) {
+    C.valid = col < NCOL;
+    const int cc = C.valid ? col : 0;
+    const int li = cc / OW, lj = cc - (cc / OW) * OW;
+    C.cxo = li - OB;
+    C.cyo = lj - OB;
+    C.iw = wrap1(i0 + C.cxo, Ng);
+    C.jw = wrap1(j0 + C.cyo, Ng);
+    C.iwf = (float) C.iw;
+    C.jwf = (float) C.jw;
+    C.base = ((size_t) C.iw * Ng + C.jw) * Ng;
+    C.own = C.valid && (unsigned) C.cxo < (unsigned) TT && (unsigned) C.cyo < (unsigned) TT;
+  };
+  Col A, B;
+  setup(threadIdx.x, A);
+  setup(threadIdx.x + TNT, B);
+  const int lane = threadIdx.x & 31;
+  auto zwrap = [&](int c) { const int z = c * CZ; return z < 0 ? z + Ng : (z >= Ng ? z - Ng : z); };
+  auto load = [&](const Col &C, int c, float4 &a, float4 &b, float4 &d) {
+    if (!C.valid) return;
+    const size_t o = C.base + zwrap(c);
+    a = *reinterpret_cast<const float4 *>(p0 + o);
+    b = *reinterpret_cast<const float4 *>(p1 + o);
+    d = *reinterpret_cast<const float4 *>(p2 + o);
+  };
+  float4 a0 = make_float4(0, 0, 0, 0), a1 = a0, a2 = a0, b0 = a0, b1 = a0, b2 = a0;
+  load(A, cfirst, a0, a1, a2);
+  load(B, cfirst, b0, b1, b2);
+  __syncthreads();
+
+  for (int c = cfirst; c <= clast; c++) {
+    // ring offsets of chunks c-1, c, c+1 (c >= -1, so c + 2 >= 1)
+    const int rb0 = ((c + 2) % 3) * (CZ * TSLOT);
+    const int rb1 = ((c + 3) % 3) * (CZ * TSLOT);
+    const int rb2 = ((c + 4) % 3) * (CZ * TSLOT);
+    const int zc = zwrap(c);
+    // one particle: lattice z (unwrapped) zu, wrapped zw
+    auto deposit = [&](const Col &C, float pa, float pb, float pc, int kz) {
+      const int zu = c * CZ + kz;
+      const float zwf = (float) (zc + kz);
+      // positions and weights as dens_field.c:262-275 (separate multiply and
+      // add in single precision; the floor of a float is exact)
+      const float x = __fadd_rn(__fmul_rn(pa, igs), C.iwf);
+      const float y = __fadd_rn(__fmul_rn(pb, igs), C.jwf);
+      const float z = __fadd_rn(__fmul_rn(pc, igs), zwf);
+      const int x0 = ffloor(x), y0 = ffloor(y), z0 = ffloor(z);
+      const int dx = x0 - C.iw, dy = y0 - C.jw, dz = z0 - (zc + kz);
+      const bool far = (unsigned) (dx + OH) > (unsigned) (2 * OH) ||
+                       (unsigned) (dy + OH) > (unsigned) (2 * OH) ||
+                       (unsigned) (dz + OH) > (unsigned) (2 * OH);
+      const bool ownp = C.own && zu >= zs && zu < ze;
+      if (OH > 2) {
+        const bool far2 = (unsigned) (dx + 2) > 4u || (unsigned) (dy + 2) > 4u ||
+                          (unsigned) (dz + 2) > 4u;
+        const unsigned f2 = __ballot_sync(0xffffffffu, far2 && ownp);
+        if (f2 && lane == __ffs(f2) - 1) atomicAdd(&stats->nfar2, (unsigned) __popc(f2));
+      }
+      const unsigned fm = __ballot_sync(0xffffffffu, far && ownp);
+      if (fm) {
+        const int leader = __ffs(fm) - 1;
+        unsigned int lb = 0;
+        if (lane == leader) {
+          lb = atomicAdd(&stats->nlist, (unsigned) __popc(fm));
+          if (OH == 2) atomicAdd(&stats->nfar2, (unsigned) __popc(fm));
+        }
+        lb = __shfl_sync(0xffffffffu, lb, leader);
+        if (far && ownp)
+          list[lb + __popc(fm & ((1u << lane) - 1))] = (unsigned int) (C.base + (zc + kz));
+      }
+      const int cx = C.cxo + dx, cy = C.cyo + dy, s = zu + dz;
+      const bool ax0 = (unsigned) cx < (unsigned) TT, ax1 = (unsigned) (cx + 1) < (unsigned) TT;
+      const bool by0 = (unsigned) cy < (unsigned) TT, by1 = (unsigned) (cy + 1) < (unsigned) TT;
+      if (far || !C.valid || !((ax0 || ax1) && (by0 || by1))) return;
+      const float wx1 = x - x0, wx0 = 1 - wx1;
+      const float wy1 = y - y0, wy0 = 1 - wy1;
+      const float wz1 = z - z0, wz0 = 1 - wz1;
+      // ring offsets (ints) of slices s and s + 1 (s >> 2 is one of c-1, c,
+      // c+1)
+      const int k0 = (s >> 2) - c, k1 = ((s + 1) >> 2) - c;
+      const int s0 = (k0 < 0 ? rb0 : (k0 == 0 ? rb1 : rb2)) + (s & (CZ - 1)) * TSLOT;
+      const int s1 = (k1 < 0 ? rb0 : (k1 == 0 ? rb1 : rb2)) + ((s + 1) & (CZ - 1)) * TSLOT;
+      const float sm1 = pa * mscale, sm2 = pb * mscale, sm3 = pc * mscale;
+      const float zr[2] = {wz0 * RHO_SCALE, wz1 * RHO_SCALE};
+      const float za[2] = {wz0 * sm1, wz1 * sm1};
+      const float zb[2] = {wz0 * sm2, wz1 * sm2};
+      const float zd[2] = {wz0 * sm3, wz1 * sm3};
+      const float wxy[4] = {wx0 * wy0, wx0 * wy1, wx1 * wy0, wx1 * wy1};
+      const bool okx[2] = {ax0, ax1}, oky[2] = {by0, by1};
+      const int ss[2] = {s0, s1};
+      const int oxy = cx * TT + cy;
+#pragma unroll
+      for (int ab = 0; ab < 4; ab++) {
+        const int ia = ab >> 1, ib = ab & 1;
+        if (!(okx[ia] && oky[ib])) continue;
+        const float w = wxy[ab];
+#pragma unroll
+        for (int ic = 0; ic < 2; ic++) {
+          int *r = tring + ss[ic] + oxy + ia * TT + ib;
+          atomicAdd(r, fmround(w, zr[ic]));
+          atomicAdd(r + TQS, fmround(w, za[ic]));
+          atomicAdd(r + 2 * TQS, fmround(w, zb[ic]));
+          atomicAdd(r + 3 * TQS, fmround(w, zd[ic]));
+        }
+      }
+    };
+    {
+      const float4 x = a0, y = a1, z = a2;
+      if (c < clast) load(A, c + 1, a0, a1, a2);
+      deposit(A, x.x, y.x, z.x, 0);
+      deposit(A, x.y, y.y, z.y, 1);
+      deposit(A, x.z, y.z, z.z, 2);
+      deposit(A, x.w, y.w, z.w, 3);
+    }
+    {
+      const float4 x = b0, y = b1, z = b2;
+      if (c < clast) load(B, c + 1, b0, b1, b2);
+      deposit(B, x.x, y.x, z.x, 0);
+      deposit(B, x.y, y.y, z.y, 1);
+      deposit(B, x.z, y.z, z.z, 2);
+      deposit(B, x.w, y.w, z.w, 3);
+    }
+    __syncthreads();
+    // chunk c-1 is complete: write it if the CTA owns it, and clear its slot
+    // for chunk c+2
+    const int o = c - 1;
+    const bool wr = o * CZ >= zs && o * CZ < ze;
+    for (int t = threadIdx.x; t < 4 * TSLOT; t += TNT) {
+      const int q = t / TSLOT, col = t - q * TSLOT;
+      int *src = tring + q * TQS + rb0 + col;
+      const int v0 = src[0], v1 = src[TSLOT], v2 = src[2 * TSLOT], v3 = src[3 * TSLOT];
+      src[0] = 0; src[TSLOT] = 0; src[2 * TSLOT] = 0; src[3 * TSLOT] = 0;
+      if (wr) {
+        const float f = (q == 0) ? (1.f / RHO_SCALE) : minv;
+        real *g = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
+        const int cx = col >> 5, cy = col & (TT - 1);
+        *reinterpret_cast<float4 *>(g + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + o * CZ) =
+            make_float4(v0 * f, v1 * f, v2 * f, v3 * f);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Deposits the listed far-displaced particles with global atomics.
 __global__ void __launch_bounds__(CIC_NT)
 fixup_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
@@ -429,13 +628,43 @@ int ez_cic(EzMesh *m, double Lbox) {
       else if (m->h_cic && cudaEventQuery(m->ev_cic) == cudaSuccess)
         m->cic_oh = ((size_t) m->h_cic[0] * 4096 < N) ? 2 : 3;
       cudaMemsetAsync(&stats->nlist, 0, 2 * sizeof(int), m->stream);
-      const unsigned nblk = (unsigned) ((Ng / OT) * (Ng / OT));
-      if (m->cic_oh != 2)
-        cic_owner_kernel<3><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
-            m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
-      else
-        cic_owner_kernel<2><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
-            m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
+      if (Ng % TT == 0 && Ng >= 2 * TT && !m->cic_legacy) {
+        // 32 x 32 tiles; the z range is cut so that the CTAs (one per SM)
+        // fill whole waves: pick the cut count with the least time per
+        // wave-slot, counting each range's two extra chunks
+        const size_t tsmem = 4 * (size_t) TQS * sizeof(int);
+        if (!EZ_CUDA_OK(cudaFuncSetAttribute(cic_tile_kernel<2>,
+                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) tsmem)) ||
+            !EZ_CUDA_OK(cudaFuncSetAttribute(cic_tile_kernel<3>,
+                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) tsmem)))
+          return EZMOCK_ERR_UNKNOWN;
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+        const long tiles = (long) (Ng / TT) * (Ng / TT);
+        int nzs = 1;
+        double best = 1e300;
+        for (int s = 1; s <= 64 && Ng / s >= 4 * CZ && (Ng / s) % CZ == 0 && Ng % s == 0; s *= 2) {
+          const long waves = (tiles * s + nsm - 1) / nsm;
+          const double cost = (double) waves * (Ng / s / CZ + 2);
+          if (cost < best * 0.999) { best = cost; nzs = s; }
+        }
+        const unsigned nblk = (unsigned) (tiles * nzs);
+        if (m->cic_oh != 2)
+          cic_tile_kernel<3><<<nblk, TNT, tsmem, m->stream>>>(m->psi[0], m->psi[1],
+              m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list, nzs);
+        else
+          cic_tile_kernel<2><<<nblk, TNT, tsmem, m->stream>>>(m->psi[0], m->psi[1],
+              m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list, nzs);
+      }
+      else {
+        const unsigned nblk = (unsigned) ((Ng / OT) * (Ng / OT));
+        if (m->cic_oh != 2)
+          cic_owner_kernel<3><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
+              m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
+        else
+          cic_owner_kernel<2><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
+              m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
+      }
       ez_count_launch();
       fixup_kernel<<<148 * 4, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
           m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs,

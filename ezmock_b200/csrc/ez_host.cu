@@ -1012,6 +1012,10 @@ int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
       m->cic_oh = (int) value;
       m->cic_oh_set = true;               // not replaced by the last field's count
       return 0;
+    case EZMOCKB200_OPT_CIC_TILE:
+      if (value != 16 && value != 32) return (*err = EZMOCK_ERR_ARG_PARAMS);
+      m->cic_legacy = value == 16;
+      return 0;
     default: return (*err = EZMOCK_ERR_ARG_PARAMS);
   }
 }

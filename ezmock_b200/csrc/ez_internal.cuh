@@ -85,6 +85,7 @@ struct EzMesh {
   int cic_mode;            // 0: float atomics, 1: deterministic fixed-point
   int cic_oh;              // halo of the owner-computes CIC (2; otherwise 3)
   bool cic_oh_set;         // cic_oh set by the caller for the next field
+  bool cic_legacy;         // FP32 CIC on 16 x 16 tiles instead of 32 x 32
 
   int Ng;
   size_t N;                // Ng^3

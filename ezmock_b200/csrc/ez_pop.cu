@@ -1253,9 +1253,17 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
   CandBuf &c = cb ? *cb : none;
   compact_kernel<<<(unsigned) ((N + CH - 1) / CH), NT, 0, st>>>(rhot, N, cut, keys_a,
       ps.counter, c.key, c.idx, c.cap, ps.cstart, ps.ccnt); ez_count_launch();
-  unsigned long long M = 0;
-  if (!EZ_CUDA_OK(cudaMemcpyAsync(&M, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
-      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+  // The candidate count is known without waiting for the compaction: a
+  // cell's histogram bin is 5 - ilogb(rho_t) (clamped), so for a cut below
+  // the last bin, bin <= imax exactly when rho_t >= 2^(5 - imax) = cut, and
+  // the candidates are the cells counted in bins 0..imax (cells that are not
+  // valid have rho_t = 0 and are in no bin).  The device counter is checked
+  // against it at the boundaries' read-back below.  With the cut in the last
+  // bin (zero and subnormal rho_t) the count is read back.
+  unsigned long long M = cnt;
+  if (imax == EZ_NLOGB - 1 &&
+      (!EZ_CUDA_OK(cudaMemcpyAsync(&M, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
+       !EZ_CUDA_OK(cudaStreamSynchronize(st))))
     return EZMOCK_ERR_UNKNOWN;
   c.ok = c.key && M <= c.cap;
   skey_t *sorted = keys_a;
@@ -1279,9 +1287,12 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
   for (int j = 0; j < nmax; j++) m->h_small[j] = pdf[j];
   cudaMemcpyAsync(ps.dpdf, m->h_small, nmax * 8, cudaMemcpyHostToDevice, st);
   bounds_kernel<<<1, 1, 0, st>>>(sorted, M, ps.dpdf, nmax, ncell, ntot, ps.bo); ez_count_launch();
+  unsigned long long Mdev = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(hb, ps.bo, sizeof(*hb), cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaMemcpyAsync(&Mdev, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
     return EZMOCK_ERR_UNKNOWN;
+  if (Mdev != M) return EZMOCK_ERR_UNKNOWN;
   return 0;
 }
 

@@ -29,6 +29,10 @@ extern "C" {
    malloc() blocks for the next catalogues (a worker thread faults them in
    while the GPU computes); 0 turns the pool off.  Default 2048. */
 #define EZMOCKB200_OPT_HOST_POOL 6
+/* Column tile of the FP32 density assignment: 32 (32 x 32 cells, the
+   default, for grids that are multiples of 32) or 16 (16 x 16 cells).  Both
+   give the same field. */
+#define EZMOCKB200_OPT_CIC_TILE 7
 
 int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     int *err);

@@ -87,3 +87,26 @@ int ezref_select_from(EZMOCK *ez, const real *rhot_in, const size_t *hist_in,
   EZmock_pdf_destroy(pdf);
   return *err;
 }
+
+/* Wall time (seconds) of the three complex-to-real FFTs that
+   EZmock_create_dens_field runs on an Ng^3 grid (perturb.c:361,397-398),
+   through the same FFTW interface and thread count, on a zeroed spectrum:
+   the FFT's share of the reference's CPU time. */
+#include <time.h>
+double ezref_fft_c2r_seconds(int Ng, int nthread) {
+  const size_t nk = (size_t) Ng * Ng * (Ng / 2 + 1);
+  FFT_CMPLX *in = FFT_MALLOC(sizeof(FFT_CMPLX) * nk);
+  FFT_REAL *out = FFT_MALLOC(sizeof(FFT_REAL) * (size_t) Ng * Ng * Ng);
+  if (!in || !out) { FFT_FREE(in); FFT_FREE(out); return -1; }
+  memset(in, 0, sizeof(FFT_CMPLX) * nk);
+  FFT_PLAN_OMP(nthread > 0 ? nthread : omp_get_max_threads());
+  FFT_PLAN p = FFT_PLAN_C2R(Ng, Ng, Ng, in, out, FFT_FLAG);
+  struct timespec t0, t1;
+  clock_gettime(CLOCK_MONOTONIC, &t0);
+  for (int d = 0; d < 3; d++) FFT_EXEC_C2R(p, in, out);
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  FFT_DESTROY(p);
+  FFT_FREE(in);
+  FFT_FREE(out);
+  return (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
+}
