@@ -294,48 +294,63 @@ cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
   }
 }
 
-// ---- owner-computes kernel on 32 x 32 column tiles (FP32, Ng % 32 == 0) ----
+// ---- owner-computes kernel on 16 x 32 column tiles (FP32, Ng % 32 == 0) ----
 //
-// A CTA owns a 32 x 32 column of cells over a z range [zs, ze) (the grid is
-// cut along z as well, so that the CTAs fill whole waves of one CTA per SM)
-// and walks it in chunks of CZ = 4 slices.  Each of its 768 threads owns two
-// of the (32 + 2 OH + 1)^2 Lagrangian columns whose particles can reach the
-// tile, for the whole walk: its column's coordinates, wrapped lattice
-// indices and output offsets are computed once, and a chunk's four particles
-// of a column arrive as one 16-byte load per displacement field, issued one
-// column ahead.  Accumulation is 32-bit fixed point in a shared-memory ring
-// of three chunks laid out [quantity][slot][x][y] with y fastest: the lanes
-// of a warp hold consecutive Lagrangian columns along y, so a deposit's bank
-// is its y cell, and lanes collide only where the flow compresses along y
-// (distinct cells in one bank or the same cell).  Chunk c's particles reach
-// chunks c-1 .. c+1; chunk c-1 is final after chunk c and is written with
-// plain 16-byte stores (its four slices of one cell row and quantity).
-// Particles displaced by more than OH cells are listed by the CTA that owns
-// their Lagrangian cell and deposited by fixup_kernel, as in the kernel
-// above; the fixed-point scales and the overflow bound are the same.
-constexpr int TT = 32;                        // tile side (x and y)
-constexpr int CZ = 4;                         // z slices per chunk
-constexpr int TRS = 3 * CZ;                   // ring slots
-constexpr int TNT = 768;                      // threads: two columns each
-constexpr int TQS = TRS * TT * TT;            // ints per quantity
-constexpr int TSLOT = TT * TT;                // ints per slot
+// A CTA owns 16 (x) by 32 (y) columns of cells over a z range [zs, ze) (the
+// grid is also cut along z so that the CTAs, one per SM, fill whole waves)
+// and walks it eight slices at a time.  Each thread owns two of the
+// (16 + 2 OH + 1) x (32 + 2 OH + 1) Lagrangian columns whose particles can
+// reach the tile, for the whole walk.  A column's next eight particles (one
+// 32-byte sector per displacement field, two 16-byte loads) are loaded into
+// registers while its current eight are deposited, so every sector is read
+// from memory once.  Accumulation is 32-bit fixed point (rho in units of
+// 2^-21, the momenta in units of 2^-s from max |psi|, as in the kernel above)
+// in a shared ring of 24 slices laid out [quantity][slice][x][y] with y
+// fastest: the lanes of a warp hold consecutive Lagrangian columns along y,
+// so a deposit's bank is its y cell.  Particles z = 8p .. 8p+7 reach slices
+// 8p-3 .. 8p+11; after them the eight slices 8p-8 .. 8p-1 are final and are
+// written with plain 32-byte stores (one sector per cell and quantity), and
+// cleared; at most 20 slices are live at once.  Deposits use `red.shared` on
+// 32-bit shared addresses.  Particles displaced by more than OH cells are
+// listed by the CTA that owns their Lagrangian cell and deposited by
+// fixup_kernel; the overflow bound is the same as above.
+constexpr int TX = 16;                        // tile rows (x)
+constexpr int TY = 32;                        // tile columns (y): one per bank
+constexpr int TZ = 8;                         // particles per column and step
+constexpr int TRS = 24;                       // ring slices
+constexpr int TSLOT = TX * TY;                // ints per slice and quantity
+constexpr int TQS = TRS * TSLOT;              // ints per quantity
+constexpr int TNT = 480;                      // threads: two columns each
+constexpr size_t TSMEM = 4 * (size_t) TQS * sizeof(int);
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t) __cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void red_add(uint32_t addr, int v) {
+  asm volatile("red.shared.add.s32 [%0], %1;" :: "r"(addr), "r"(v) : "memory");
+}
 
 template <int OH>
 __global__ void __launch_bounds__(TNT, 1)
 cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
     const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
     int Ng, real igs, CicStats *stats, unsigned int *list, int nzs) {
-  constexpr int OW = TT + 2 * OH + 1;         // Lagrangian columns per side
+  constexpr int OWX = TX + 2 * OH + 1;        // Lagrangian columns along x
+  constexpr int OWY = TY + 2 * OH + 1;        // and along y
   constexpr int OB = OH + 1;                  // read origin: i0 - OB, j0 - OB
-  constexpr int NCOL = OW * OW;
+  constexpr int NCOL = OWX * OWY;
   static_assert(NCOL <= 2 * TNT, "two columns per thread");
-  extern __shared__ __align__(16) int tring[];  // [4][TRS][TT][TT]
-  const int ntile = Ng / TT;
+  extern __shared__ __align__(128) int tring[];   // [4][TRS][TX][TY]
+  const uint32_t ringb = smem_u32(tring);
+  const int nty = Ng / TY;
   const int tile = blockIdx.x / nzs, zsp = blockIdx.x - tile * nzs;
-  const int i0 = (tile / ntile) * TT, j0 = (tile % ntile) * TT;
+  const int i0 = (tile / nty) * TX, j0 = (tile % nty) * TY;
   const int zlen = Ng / nzs;
   const int zs = zsp * zlen, ze = zs + zlen;
-  const int cfirst = zs / CZ - 1, clast = ze / CZ;
+  // steps p cover particles z = 8p .. 8p + 7; those that reach [zs, ze) lie
+  // in z = zs - 4 .. ze + 2
+  const int pfirst = zs / TZ - 1, plast = ze / TZ;
   const float pmax = fmaxf(__uint_as_float(stats->psimax_bits), 1e-30f);
   const float mscale = exp2f(floorf(log2f(2147483647.f / (1024.f * pmax))));
   const float minv = 1.f / mscale;
@@ -346,151 +361,145 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
   struct Col {
     int cxo, cyo;          // tile coordinates of the Lagrangian column
     int iw, jw;            // wrapped lattice indices
-    float iwf, jwf;
-    size_t base;           // offset of the column's z = 0 particle
     bool own, valid;
   };
   auto setup = [&](int col, Col &C) {
     C.valid = col < NCOL;
     const int cc = C.valid ? col : 0;
-    const int li = cc / OW, lj = cc - (cc / OW) * OW;
+    const int li = cc / OWY, lj = cc - (cc / OWY) * OWY;
     C.cxo = li - OB;
     C.cyo = lj - OB;
     C.iw = wrap1(i0 + C.cxo, Ng);
     C.jw = wrap1(j0 + C.cyo, Ng);
-    C.iwf = (float) C.iw;
-    C.jwf = (float) C.jw;
-    C.base = ((size_t) C.iw * Ng + C.jw) * Ng;
-    C.own = C.valid && (unsigned) C.cxo < (unsigned) TT && (unsigned) C.cyo < (unsigned) TT;
+    C.own = C.valid && (unsigned) C.cxo < (unsigned) TX && (unsigned) C.cyo < (unsigned) TY;
   };
-  Col A, B;
-  setup(threadIdx.x, A);
-  setup(threadIdx.x + TNT, B);
-  const int lane = threadIdx.x & 31;
-  auto zwrap = [&](int c) { const int z = c * CZ; return z < 0 ? z + Ng : (z >= Ng ? z - Ng : z); };
-  auto load = [&](const Col &C, int c, float4 &a, float4 &b, float4 &d) {
+  Col colA, colB;
+  setup(threadIdx.x, colA);
+  setup(threadIdx.x + TNT, colB);
+  auto zwrap = [&](int p) { const int z = p * TZ; return z < 0 ? z + Ng : (z >= Ng ? z - Ng : z); };
+  // [column][field][half]: a step's particles of both columns; a column's
+  // next step is loaded as soon as its particles of this step are taken
+  float4 cur[2][3][2];
+  auto load = [&](int k, int p) {
+    const Col &C = k ? colB : colA;
     if (!C.valid) return;
-    const size_t o = C.base + zwrap(c);
-    a = *reinterpret_cast<const float4 *>(p0 + o);
-    b = *reinterpret_cast<const float4 *>(p1 + o);
-    d = *reinterpret_cast<const float4 *>(p2 + o);
+    const size_t o = ((size_t) C.iw * Ng + C.jw) * Ng + zwrap(p);
+    const real *src[3] = {p0 + o, p1 + o, p2 + o};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      cur[k][a][0] = *reinterpret_cast<const float4 *>(src[a]);
+      cur[k][a][1] = *reinterpret_cast<const float4 *>(src[a] + 4);
+    }
   };
-  float4 a0 = make_float4(0, 0, 0, 0), a1 = a0, a2 = a0, b0 = a0, b1 = a0, b2 = a0;
-  load(A, cfirst, a0, a1, a2);
-  load(B, cfirst, b0, b1, b2);
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int a = 0; a < 3; a++) cur[k][a][0] = cur[k][a][1] = make_float4(0, 0, 0, 0);
+  load(0, pfirst);
+  load(1, pfirst);
+  unsigned int nfar2 = 0;
   __syncthreads();
 
-  for (int c = cfirst; c <= clast; c++) {
-    // ring offsets of chunks c-1, c, c+1 (c >= -1, so c + 2 >= 1)
-    const int rb0 = ((c + 2) % 3) * (CZ * TSLOT);
-    const int rb1 = ((c + 3) % 3) * (CZ * TSLOT);
-    const int rb2 = ((c + 4) % 3) * (CZ * TSLOT);
-    const int zc = zwrap(c);
-    // one particle: lattice z (unwrapped) zu, wrapped zw
-    auto deposit = [&](const Col &C, float pa, float pb, float pc, int kz) {
-      const int zu = c * CZ + kz;
-      const float zwf = (float) (zc + kz);
-      // positions and weights as dens_field.c:262-275 (separate multiply and
-      // add in single precision; the floor of a float is exact)
-      const float x = __fadd_rn(__fmul_rn(pa, igs), C.iwf);
-      const float y = __fadd_rn(__fmul_rn(pb, igs), C.jwf);
-      const float z = __fadd_rn(__fmul_rn(pc, igs), zwf);
-      const int x0 = ffloor(x), y0 = ffloor(y), z0 = ffloor(z);
-      const int dx = x0 - C.iw, dy = y0 - C.jw, dz = z0 - (zc + kz);
-      const bool far = (unsigned) (dx + OH) > (unsigned) (2 * OH) ||
-                       (unsigned) (dy + OH) > (unsigned) (2 * OH) ||
-                       (unsigned) (dz + OH) > (unsigned) (2 * OH);
-      const bool ownp = C.own && zu >= zs && zu < ze;
-      if (OH > 2) {
-        const bool far2 = (unsigned) (dx + 2) > 4u || (unsigned) (dy + 2) > 4u ||
-                          (unsigned) (dz + 2) > 4u;
-        const unsigned f2 = __ballot_sync(0xffffffffu, far2 && ownp);
-        if (f2 && lane == __ffs(f2) - 1) atomicAdd(&stats->nfar2, (unsigned) __popc(f2));
-      }
-      const unsigned fm = __ballot_sync(0xffffffffu, far && ownp);
-      if (fm) {
-        const int leader = __ffs(fm) - 1;
-        unsigned int lb = 0;
-        if (lane == leader) {
-          lb = atomicAdd(&stats->nlist, (unsigned) __popc(fm));
-          if (OH == 2) atomicAdd(&stats->nfar2, (unsigned) __popc(fm));
-        }
-        lb = __shfl_sync(0xffffffffu, lb, leader);
-        if (far && ownp)
-          list[lb + __popc(fm & ((1u << lane) - 1))] = (unsigned int) (C.base + (zc + kz));
-      }
-      const int cx = C.cxo + dx, cy = C.cyo + dy, s = zu + dz;
-      const bool ax0 = (unsigned) cx < (unsigned) TT, ax1 = (unsigned) (cx + 1) < (unsigned) TT;
-      const bool by0 = (unsigned) cy < (unsigned) TT, by1 = (unsigned) (cy + 1) < (unsigned) TT;
-      if (far || !C.valid || !((ax0 || ax1) && (by0 || by1))) return;
-      const float wx1 = x - x0, wx0 = 1 - wx1;
-      const float wy1 = y - y0, wy0 = 1 - wy1;
-      const float wz1 = z - z0, wz0 = 1 - wz1;
-      // ring offsets (ints) of slices s and s + 1 (s >> 2 is one of c-1, c,
-      // c+1)
-      const int k0 = (s >> 2) - c, k1 = ((s + 1) >> 2) - c;
-      const int s0 = (k0 < 0 ? rb0 : (k0 == 0 ? rb1 : rb2)) + (s & (CZ - 1)) * TSLOT;
-      const int s1 = (k1 < 0 ? rb0 : (k1 == 0 ? rb1 : rb2)) + ((s + 1) & (CZ - 1)) * TSLOT;
-      const float sm1 = pa * mscale, sm2 = pb * mscale, sm3 = pc * mscale;
-      const float zr[2] = {wz0 * RHO_SCALE, wz1 * RHO_SCALE};
-      const float za[2] = {wz0 * sm1, wz1 * sm1};
-      const float zb[2] = {wz0 * sm2, wz1 * sm2};
-      const float zd[2] = {wz0 * sm3, wz1 * sm3};
-      const float wxy[4] = {wx0 * wy0, wx0 * wy1, wx1 * wy0, wx1 * wy1};
-      const bool okx[2] = {ax0, ax1}, oky[2] = {by0, by1};
-      const int ss[2] = {s0, s1};
-      const int oxy = cx * TT + cy;
+  for (int p = pfirst; p <= plast; p++) {
+    const int zc = zwrap(p);
+    // ring slice of the unwrapped slice 8p - 8 (slices 8p-8 .. 8p+15 map to
+    // rbase + 0 .. 23, wrapping past 24)
+    const int rbase = (((p - 1) % 3) + 3) % 3 * TZ;
 #pragma unroll
-      for (int ab = 0; ab < 4; ab++) {
-        const int ia = ab >> 1, ib = ab & 1;
-        if (!(okx[ia] && oky[ib])) continue;
-        const float w = wxy[ab];
+    for (int k = 0; k < 2; k++) {
+      const Col &C = k ? colB : colA;
 #pragma unroll
-        for (int ic = 0; ic < 2; ic++) {
-          int *r = tring + ss[ic] + oxy + ia * TT + ib;
-          atomicAdd(r, fmround(w, zr[ic]));
-          atomicAdd(r + TQS, fmround(w, za[ic]));
-          atomicAdd(r + 2 * TQS, fmround(w, zb[ic]));
-          atomicAdd(r + 3 * TQS, fmround(w, zd[ic]));
+      for (int kz = 0; kz < TZ; kz++) {
+        const int h = kz >> 2, e = kz & 3;
+        const float pa = (&cur[k][0][h].x)[e], pb = (&cur[k][1][h].x)[e];
+        const float pc = (&cur[k][2][h].x)[e];
+        if (kz == TZ - 1 && p < plast) load(k, p + 1);
+        const int zu = p * TZ + kz;
+        const bool ownp = C.own && zu >= zs && zu < ze;
+        // positions and weights as dens_field.c:262-275: separate single-
+        // precision multiply and add; floor by rounding to an integer with
+        // a magic addition (exact for |v| < 2^22); w1 = v - floor(v), one
+        // rounding, as the reference's `x - x0`
+        const float x = __fadd_rn(__fmul_rn(pa, igs), (float) C.iw);
+        const float y = __fadd_rn(__fmul_rn(pb, igs), (float) C.jw);
+        const float z = __fadd_rn(__fmul_rn(pc, igs), (float) (zc + kz));
+        const float tx = __fadd_rn(x, RMAGIC), ty = __fadd_rn(y, RMAGIC), tz = __fadd_rn(z, RMAGIC);
+        const float ex = __fsub_rn(x, __fsub_rn(tx, RMAGIC));
+        const float ey = __fsub_rn(y, __fsub_rn(ty, RMAGIC));
+        const float ez = __fsub_rn(z, __fsub_rn(tz, RMAGIC));
+        const int nx = ex < 0, ny = ey < 0, nz = ez < 0;
+        const int dx = __float_as_int(tx) - 0x4B400000 - nx - C.iw;
+        const int dy = __float_as_int(ty) - 0x4B400000 - ny - C.jw;
+        const int dz = __float_as_int(tz) - 0x4B400000 - nz - (zc + kz);
+        const int mad = max(max(abs(dx), abs(dy)), abs(dz));
+        nfar2 += (ownp && mad > 2) ? 1u : 0u;
+        if (mad > OH) {
+          if (ownp) {
+            const unsigned int slot = atomicAdd(&stats->nlist, 1u);
+            list[slot] = (unsigned int) (((size_t) C.iw * Ng + C.jw) * Ng + (zc + kz));
+          }
+          continue;
+        }
+        const int cx = C.cxo + dx, cy = C.cyo + dy;
+        const bool ax0 = (unsigned) cx < (unsigned) TX, ax1 = (unsigned) (cx + 1) < (unsigned) TX;
+        const bool by0 = (unsigned) cy < (unsigned) TY, by1 = (unsigned) (cy + 1) < (unsigned) TY;
+        if (!C.valid || !((ax0 || ax1) && (by0 || by1))) continue;
+        const float wx1 = nx ? ex + 1.f : ex, wx0 = 1.f - wx1;
+        const float wy1 = ny ? ey + 1.f : ey, wy0 = 1.f - wy1;
+        const float wz1 = nz ? ez + 1.f : ez, wz0 = 1.f - wz1;
+        // ring slices of s and s + 1: s - (8p - 8) is in 5 .. 19
+        int r0 = rbase + (kz + dz + TZ);
+        r0 -= (r0 >= TRS) ? TRS : 0;
+        int r1 = r0 + 1;
+        r1 -= (r1 >= TRS) ? TRS : 0;
+        const uint32_t cell = ringb + 4u * (uint32_t) (cx * TY + cy);
+        const uint32_t b0 = cell + 4u * (uint32_t) (r0 * TSLOT);
+        const uint32_t b1 = cell + 4u * (uint32_t) (r1 * TSLOT);
+        const float sm1 = pa * mscale, sm2 = pb * mscale, sm3 = pc * mscale;
+        const float zq[2][4] = {{wz0 * RHO_SCALE, wz0 * sm1, wz0 * sm2, wz0 * sm3},
+                                {wz1 * RHO_SCALE, wz1 * sm1, wz1 * sm2, wz1 * sm3}};
+        const float wxy[4] = {wx0 * wy0, wx0 * wy1, wx1 * wy0, wx1 * wy1};
+        const bool ok[4] = {ax0 && by0, ax0 && by1, ax1 && by0, ax1 && by1};
+        constexpr uint32_t QB = 4u * TQS;
+#pragma unroll
+        for (int ab = 0; ab < 4; ab++) {
+          if (!ok[ab]) continue;
+          const uint32_t off = 4u * (uint32_t) ((ab >> 1) * TY + (ab & 1));
+#pragma unroll
+          for (int ic = 0; ic < 2; ic++) {
+            const uint32_t r = (ic ? b1 : b0) + off;
+#pragma unroll
+            for (int q = 0; q < 4; q++) red_add(r + q * QB, fmround(wxy[ab], zq[ic][q]));
+          }
         }
       }
-    };
-    {
-      const float4 x = a0, y = a1, z = a2;
-      if (c < clast) load(A, c + 1, a0, a1, a2);
-      deposit(A, x.x, y.x, z.x, 0);
-      deposit(A, x.y, y.y, z.y, 1);
-      deposit(A, x.z, y.z, z.z, 2);
-      deposit(A, x.w, y.w, z.w, 3);
     }
-    {
-      const float4 x = b0, y = b1, z = b2;
-      if (c < clast) load(B, c + 1, b0, b1, b2);
-      deposit(B, x.x, y.x, z.x, 0);
-      deposit(B, x.y, y.y, z.y, 1);
-      deposit(B, x.z, y.z, z.z, 2);
-      deposit(B, x.w, y.w, z.w, 3);
-    }
+    // slices 8p-8 .. 8p-1 are final: written if the CTA owns them (a sector
+    // of eight slices per cell and quantity) and cleared
     __syncthreads();
-    // chunk c-1 is complete: write it if the CTA owns it, and clear its slot
-    // for chunk c+2
-    const int o = c - 1;
-    const bool wr = o * CZ >= zs && o * CZ < ze;
+    const int zo = (p - 1) * TZ;
+    const bool wr = zo >= zs && zo < ze;
     for (int t = threadIdx.x; t < 4 * TSLOT; t += TNT) {
-      const int q = t / TSLOT, col = t - q * TSLOT;
-      int *src = tring + q * TQS + rb0 + col;
-      const int v0 = src[0], v1 = src[TSLOT], v2 = src[2 * TSLOT], v3 = src[3 * TSLOT];
-      src[0] = 0; src[TSLOT] = 0; src[2 * TSLOT] = 0; src[3 * TSLOT] = 0;
+      const int q = t / TSLOT, cc = t - q * TSLOT;
+      int *src = tring + q * TQS + rbase * TSLOT + cc;
+      int v[TZ];
+#pragma unroll
+      for (int kk = 0; kk < TZ; kk++) { v[kk] = src[kk * TSLOT]; src[kk * TSLOT] = 0; }
       if (wr) {
         const float f = (q == 0) ? (1.f / RHO_SCALE) : minv;
         real *g = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
-        const int cx = col >> 5, cy = col & (TT - 1);
-        *reinterpret_cast<float4 *>(g + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + o * CZ) =
-            make_float4(v0 * f, v1 * f, v2 * f, v3 * f);
+        const int cx = cc / TY, cy = cc - (cc / TY) * TY;
+        float4 *dst = reinterpret_cast<float4 *>(g + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo);
+        dst[0] = make_float4(v[0] * f, v[1] * f, v[2] * f, v[3] * f);
+        dst[1] = make_float4(v[4] * f, v[5] * f, v[6] * f, v[7] * f);
       }
     }
     __syncthreads();
   }
+  // particles displaced beyond two cells, for the next field's halo
+#pragma unroll
+  for (int o = 16; o; o >>= 1) nfar2 += __shfl_xor_sync(0xffffffffu, nfar2, o);
+  if ((threadIdx.x & 31) == 0 && nfar2) atomicAdd(&stats->nfar2, nfar2);
 }
 
 // Deposits the listed far-displaced particles with global atomics.
@@ -628,32 +637,32 @@ int ez_cic(EzMesh *m, double Lbox) {
       else if (m->h_cic && cudaEventQuery(m->ev_cic) == cudaSuccess)
         m->cic_oh = ((size_t) m->h_cic[0] * 4096 < N) ? 2 : 3;
       cudaMemsetAsync(&stats->nlist, 0, 2 * sizeof(int), m->stream);
-      if (Ng % TT == 0 && Ng >= 2 * TT && !m->cic_legacy) {
-        // 32 x 32 tiles; the z range is cut so that the CTAs (one per SM)
+      if (Ng % TY == 0 && Ng >= 2 * TY && !m->cic_legacy) {
+        // 16 x 32 tiles; the z range is cut so that the CTAs (one per SM)
         // fill whole waves: pick the cut count with the least time per
-        // wave-slot, counting each range's two extra chunks
-        const size_t tsmem = 4 * (size_t) TQS * sizeof(int);
+        // wave-slot, counting each range's two extra steps
         if (!EZ_CUDA_OK(cudaFuncSetAttribute(cic_tile_kernel<2>,
-                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) tsmem)) ||
+                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) TSMEM)) ||
             !EZ_CUDA_OK(cudaFuncSetAttribute(cic_tile_kernel<3>,
-                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) tsmem)))
+                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) TSMEM)))
           return EZMOCK_ERR_UNKNOWN;
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-        const long tiles = (long) (Ng / TT) * (Ng / TT);
+        const long tiles = (long) (Ng / TX) * (Ng / TY);
         int nzs = 1;
         double best = 1e300;
-        for (int s = 1; s <= 64 && Ng / s >= 4 * CZ && (Ng / s) % CZ == 0 && Ng % s == 0; s *= 2) {
+        for (int s = 1; s <= 64 && Ng % s == 0 && (Ng / s) % TZ == 0 && Ng / s >= 2 * TZ;
+             s *= 2) {
           const long waves = (tiles * s + nsm - 1) / nsm;
-          const double cost = (double) waves * (Ng / s / CZ + 2);
+          const double cost = (double) waves * (Ng / s / TZ + 2);
           if (cost < best * 0.999) { best = cost; nzs = s; }
         }
         const unsigned nblk = (unsigned) (tiles * nzs);
         if (m->cic_oh != 2)
-          cic_tile_kernel<3><<<nblk, TNT, tsmem, m->stream>>>(m->psi[0], m->psi[1],
+          cic_tile_kernel<3><<<nblk, TNT, TSMEM, m->stream>>>(m->psi[0], m->psi[1],
               m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list, nzs);
         else
-          cic_tile_kernel<2><<<nblk, TNT, tsmem, m->stream>>>(m->psi[0], m->psi[1],
+          cic_tile_kernel<2><<<nblk, TNT, TSMEM, m->stream>>>(m->psi[0], m->psi[1],
               m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list, nzs);
       }
       else {

@@ -17,10 +17,12 @@ OpenMP) on the same seed and parameters.
   shifts the Gaussians of every later valid cell and the two catalogues
   become different draws of the bias noise on the same density field (the
   reference's own FP32 build behaves the same).  Tolerances: the band power
-  over all 40 bins (mode-weighted P0, and P2 relative to it) within 0.5% for
-  every seed; per bin, the seed-averaged relative P0 difference within 6
-  standard deviations of the tracer-sampling noise of one bin (its measured
-  scatter over the 40 bins and 4 seeds is printed).
+  over all 40 bins (mode-weighted P0, and P2 relative to it), averaged over
+  the four seeds, within 0.5%, and within 1% for every seed (one seed's
+  difference is a draw of the tracer-sampling noise, about 0.3% for this
+  band); per bin, the seed-averaged relative P0 difference within 6 standard
+  deviations of the sampling noise of one bin (its measured scatter over the
+  40 bins and 4 seeds is printed).
 """
 import numpy as np
 import pytest
@@ -144,8 +146,8 @@ def test_config_512_fp32_vs_fp64():
                           kmin=kmin, kmax=kmax, nbin=nbin)
         has = p64["nmodes"] > 0
         nmodes = p64["nmodes"]
-        band0 = abs(np.sum(nmodes * (p32["P0"] - p64["P0"]))) / np.sum(nmodes * p64["P0"])
-        band2 = abs(np.sum(nmodes * (p32["P2"] - p64["P2"]))) / np.sum(nmodes * p64["P0"])
+        band0 = np.sum(nmodes * (p32["P0"] - p64["P0"])) / np.sum(nmodes * p64["P0"])
+        band2 = np.sum(nmodes * (p32["P2"] - p64["P2"])) / np.sum(nmodes * p64["P0"])
         r0 = np.where(has, (p32["P0"] - p64["P0"]) / np.where(has, p64["P0"], 1), 0)
         rel0.append(r0)
         rows.append((seed, err, near, cross, occ, diff, len(cat32[0]), len(cat64[0]),
@@ -157,19 +159,23 @@ def test_config_512_fp32_vs_fp64():
           "band P0 | band P2")
     for r in rows:
         print(f"{r[0]} | {r[1]:.2e} | {r[2]} | {r[3]} | {r[4]} | {r[5]} | {r[6]} | {r[7]} | "
-              f"{100 * r[8]:.2f}% / {100 * r[9]:.1f}% | {100 * r[10]:.3f}% | {100 * r[11]:.3f}%")
+              f"{100 * r[8]:.2f}% / {100 * r[9]:.1f}% | {100 * r[10]:+.3f}% | {100 * r[11]:+.3f}%")
+    mean0 = float(np.mean([r[10] for r in rows]))
+    mean2 = float(np.mean([r[11] for r in rows]))
+    print(f"band power over seeds: P0 {100 * mean0:+.3f}%, P2 {100 * mean2:+.3f}% of P0")
+    assert abs(mean0) <= 5e-3 and abs(mean2) <= 5e-3
     for r in rows:
-        assert r[10] <= 5e-3 and r[11] <= 5e-3
+        assert abs(r[10]) <= 1e-2 and abs(r[11]) <= 1e-2
     rel0 = np.array(rel0)
     has = nmodes > 0
-    mean0 = rel0.mean(axis=0)
+    bins0 = rel0.mean(axis=0)
     # per-bin scatter of one seed's relative difference, from the 4 x 40
     # values scaled by the bin's mode count (the noise goes as 1/sqrt(modes))
     z = rel0[:, has] * np.sqrt(nmodes[has])
     sigma_unit = float(np.sqrt(np.mean(z ** 2)))
     sig_mean = sigma_unit / np.sqrt(nmodes[has]) / np.sqrt(rel0.shape[0])
-    worst = float(np.abs(mean0[has] / sig_mean).max())
+    worst = float(np.abs(bins0[has] / sig_mean).max())
     print(f"per-bin scatter: {sigma_unit:.3f} / sqrt(modes); seed-averaged P0 difference at "
           f"most {worst:.2f} standard deviations; mean over bins "
-          f"{100 * float(mean0[has].mean()):.3f}%")
+          f"{100 * float(bins0[has].mean()):.3f}%")
     assert worst <= 6.0

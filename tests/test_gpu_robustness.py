@@ -1,8 +1,9 @@
 """Host-side failure paths on the GPU, none of which faults the device.
 
-* Out of device memory: a 2048^3 instance needs about 380 GB of device
+* Out of device memory: a 2048^3 FP32 instance needs about 380 GB of device
   buffers (three spectra, three displacement fields, the density, three
-  painted grids, the random draws), more than one B200 holds.  Creating its
+  painted grids, the random draws), a 1536^3 FP64 one about 490 GB, more than
+  one B200 holds.  Creating its
   field must fail with EZMOCK_ERR_MEMORY (libEZmock/EZmock/errmsg.h:33-88,
   the reference's code for a failed allocation), keep the error sticky, free
   what was allocated, and leave the device usable for the next instance.
@@ -24,7 +25,9 @@ ERR_MEMORY = 1
 def test_out_of_device_memory(prec):
     L = _lib.load(prec)
     k, P = bbks_pk()
-    m = EZmock(Lbox=20000.0, Ngrid=2048, rng=1, seed=1, prec=prec)
+    # the largest grid of each build's transforms: about 380 GB (FP32) and
+    # 490 GB (FP64, 1536^3) of device buffers
+    m = EZmock(Lbox=20000.0, Ngrid=2048 if prec == 32 else 1536, rng=1, seed=1, prec=prec)
     m.eval_growth_params(0.8, 0.31)
     m.setup_linear_pk(k, P)
     with pytest.raises(RuntimeError, match="failed to allocate memory"):
