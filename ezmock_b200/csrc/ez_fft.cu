@@ -23,6 +23,7 @@
 //            complex FFT (even/odd packing), written as psi rows.
 // Traffic: S read once; 2 + 3 spectra written, 5 read; 3 real fields written.
 #include "ez_internal.cuh"
+#include "ez_tma.cuh"
 
 #include <cuda_pipeline.h>
 
@@ -416,6 +417,103 @@ __device__ __forceinline__ void warp_fft(cplx *v, const cplx *tw, int lane) {
   }
 }
 
+// Line transform with one pass through shared memory instead of five
+// shuffle stages.  With n = 32 E, x[l + 32 m] (lane l, m < E):
+//   Y[l][k]   = sum_m x[l + 32 m] W_E^(m k)          (E-point DFT, registers)
+//   Z[l][k]   = Y[l][k] W_n^(l k)
+//   X[k + E p] = sum_l Z[l][k] W_32^(l p),   p = q + E r,  l = G j + s (G = 32/E):
+//             = sum_s W_G^(s r) [W_32^(s q) sum_j Z[G j + s][k] W_E^(j q)].
+// Z goes through the caller's line buffer (n elements, used as scratch:
+// lane (k, s) then reads its E values Z[G j + s][k]); the inner sum over j
+// is a second register DFT, and the G-point DFT over s runs across the lanes
+// that share k, in log2 G shuffle stages (none for E = 32, one for E = 16).
+// Lane t then holds X[k(t) + E q + E^2 r(t)] for q < E, r(t) the bit-
+// reversed s(t).  The lane mapping and the scratch positions are chosen per
+// E so that the scratch writes and reads and the callers' stores to their
+// swizzled tiles are free of bank conflicts (E = 4: two-way on the stores).
+template <int E> struct W2 {
+  static constexpr int G = 32 / E;
+  static constexpr bool SHIGH = E >= 16;          // s in the high lane bits
+  static __device__ __forceinline__ int k_of(int t) { return SHIGH ? (t & (E - 1)) : (t / G); }
+  static __device__ __forceinline__ int s_of(int t) { return SHIGH ? (t / E) : (t & (G - 1)); }
+  static __device__ __forceinline__ int pos(int l, int k) {
+    return 32 * k + (l ^ (SHIGH ? k : ((G * k) & 31)));
+  }
+  static __host__ __device__ constexpr int lane_xor(int h) { return SHIGH ? h * E : h; }
+  // output index held in register q by lane t
+  static __device__ __forceinline__ int out(int t, int q) {
+    int r = 0;
+    const int s = s_of(t);
+#pragma unroll
+    for (int b = 1; b < G; b <<= 1) r = (r << 1) | ((s & b) ? 1 : 0);
+    return k_of(t) + E * q + E * E * r;
+  }
+};
+
+template <int E, int S>
+__device__ __forceinline__ void warp_fft2(cplx *v, const cplx *tw, int lane, cplx *line) {
+  typedef W2<E> M;
+  constexpr int G = M::G;
+  RegDft<E, S>::run(v);
+#pragma unroll
+  for (int k = 1; k < E; k++) {
+    cplx w = tw[lane * k];
+    if (S < 0) w.y = -w.y;
+    v[k] = cmul(v[k], w);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < E; k++) line[M::pos(lane, k)] = v[k];
+  __syncwarp();
+  const int kt = M::k_of(lane), st = M::s_of(lane);
+#pragma unroll
+  for (int j = 0; j < E; j++) v[j] = line[M::pos(G * j + st, kt)];
+  __syncwarp();
+  RegDft<E, S>::run(v);
+  if (G > 1) {
+#pragma unroll
+    for (int q = 1; q < E; q++) v[q] = cmul(v[q], w32<S>(st * q));
+  }
+  // G-point decimation-in-frequency over s across the lanes sharing k: the
+  // lower lane keeps v + b, the upper one (b - v) W_2h^(s mod h)
+#pragma unroll
+  for (int h = G / 2; h >= 1; h >>= 1) {
+    const bool hi = (st & h) != 0;
+    const rt sg = hi ? (rt) -1 : (rt) 1;
+    cplx w = w32<S>((st & (h - 1)) * (16 / h));
+    if (!hi) { w.x = 1; w.y = 0; }
+#pragma unroll
+    for (int q = 0; q < E; q++) {
+      const cplx b = shfl_xor_c(v[q], M::lane_xor(h));
+      cplx t;
+      t.x = fma(sg, v[q].x, b.x);
+      t.y = fma(sg, v[q].y, b.y);
+      v[q] = cmul(t, w);
+    }
+  }
+}
+
+// The transform a line of a tile goes through, with the output index of
+// register q of lane t: the transposed form above (T = true, single
+// precision only) or the five shuffle stages (lane t then holds
+// X[q + E brev5(t)]).  Measured per pass at 512^3 and 1024^3: the
+// transposed form pays where it removes four or five shuffle stages (E = 16
+// in passes I and K, E = 32 in pass J), and costs where it adds register
+// pressure (pass J at E = 16) or removes only three (E = 8); double
+// precision keeps the shuffles (twice the registers per value).
+template <int E> __host__ __device__ constexpr bool use_t(int pass) {
+  return sizeof(rt) == 4 && (pass == 1 ? E >= 32 : E >= 16);
+}
+template <int E, int S, bool T>
+__device__ __forceinline__ void line_fft(cplx *v, const cplx *tw, int lane, cplx *line) {
+  if (T) warp_fft2<E, S>(v, tw, lane, line);
+  else { warp_fft<E, S>(v, tw, lane); __syncwarp(); }
+}
+template <int E, bool T>
+__device__ __forceinline__ int line_out(int lane, int q) {
+  return T ? W2<E>::out(lane, q) : q + E * brev5(lane);
+}
+
 __device__ __forceinline__ int swz(int m) { return m ^ ((m >> 4) & 15); }
 
 constexpr int WNW = 8;                       // warps per block
@@ -453,7 +551,6 @@ wpass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0
   __pipeline_commit();
   __pipeline_wait_prior(0);
   __syncthreads();
-  const int r = brev5(lane);
   for (int c = w; c < WK; c += WNW) {
     cplx v[E];
 #pragma unroll
@@ -464,15 +561,14 @@ wpass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0
       v[m].x *= f;
       v[m].y *= f;
     }
-    warp_fft<E, 1>(v, tw, lane);
+    line_fft<E, 1, use_t<E>(0)>(v, tw, lane, b1 + c * LS);
 #pragma unroll
-    for (int k = 0; k < E; k++) b1[c * LS + swz(k + E * r)] = v[k];
+    for (int q = 0; q < E; q++) b1[c * LS + swz(line_out<E, use_t<E>(0)>(lane, q))] = v[q];
 #pragma unroll
     for (int m = 0; m < E; m++) v[m] = b0[c * LS + swz(32 * m + lane)];
-    warp_fft<E, 1>(v, tw, lane);
-    __syncwarp();
+    line_fft<E, 1, use_t<E>(0)>(v, tw, lane, b0 + c * LS);
 #pragma unroll
-    for (int k = 0; k < E; k++) b0[c * LS + swz(k + E * r)] = v[k];
+    for (int q = 0; q < E; q++) b0[c * LS + swz(line_out<E, use_t<E>(0)>(lane, q))] = v[q];
   }
   __syncthreads();
 #pragma unroll 4
@@ -516,15 +612,13 @@ wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
   __pipeline_commit();
   __pipeline_wait_prior(1);
   __syncthreads();
-  const int r = brev5(lane);
   for (int c = w; c < WK; c += WNW) {
     cplx v[E];
 #pragma unroll
     for (int m = 0; m < E; m++) v[m] = bx[c * LS + swz(32 * m + lane)];
-    warp_fft<E, 1>(v, tw, lane);
-    __syncwarp();
+    line_fft<E, 1, use_t<E>(1)>(v, tw, lane, bx + c * LS);
 #pragma unroll
-    for (int k = 0; k < E; k++) bx[c * LS + swz(k + E * r)] = v[k];
+    for (int q = 0; q < E; q++) bx[c * LS + swz(line_out<E, use_t<E>(1)>(lane, q))] = v[q];
   }
   __pipeline_wait_prior(0);
   __syncthreads();
@@ -538,15 +632,14 @@ wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
       v[m].x *= f;
       v[m].y *= f;
     }
-    warp_fft<E, 1>(v, tw, lane);
+    line_fft<E, 1, use_t<E>(1)>(v, tw, lane, by + c * LS);
 #pragma unroll
-    for (int k = 0; k < E; k++) by[c * LS + swz(k + E * r)] = v[k];
+    for (int q = 0; q < E; q++) by[c * LS + swz(line_out<E, use_t<E>(1)>(lane, q))] = v[q];
 #pragma unroll
     for (int m = 0; m < E; m++) v[m] = b0[c * LS + swz(32 * m + lane)];
-    warp_fft<E, 1>(v, tw, lane);
-    __syncwarp();
+    line_fft<E, 1, use_t<E>(1)>(v, tw, lane, b0 + c * LS);
 #pragma unroll
-    for (int k = 0; k < E; k++) b0[c * LS + swz(k + E * r)] = v[k];
+    for (int q = 0; q < E; q++) b0[c * LS + swz(line_out<E, use_t<E>(1)>(lane, q))] = v[q];
   }
   __syncthreads();
 #pragma unroll 4
@@ -556,6 +649,188 @@ wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
     s1[g] = bx[c * LS + swz(j)];
     s0[g] = by[c * LS + swz(j)];
     s2[g] = b0[c * LS + swz(j)];
+  }
+}
+
+// ------------------------------------------------ TMA-staged passes I, J --
+//
+// FP32, Ng = 32 E with E = 8 or 16.  The same transforms as wpass_i/j, with
+// tiles of WK = 8 columns moved by the Tensor Memory Accelerator: a tile is
+// Ng rows (i in pass I, j in pass J) of 64 bytes, copied by 256-row boxes of
+// a tensor map over the spectrum (floats, 2 Nkp x Ng x Ng) with the 64-byte
+// swizzle, so that a warp reading one column (one line) meets each bank at
+// most twice.  A persistent CTA per SM runs a two-stage pipeline: one
+// producer warp issues the loads of tile t + 2 and the stores of tile t from
+// shared memory, eight compute warps transform tile t + 1 (one column each,
+// the transposed line form warp_fft2 with a per-warp scratch line).  Pass I
+// reads S and writes A_0 in place of it and A_x through a separate tile;
+// pass J reads A_x and A_0, writes B_x and B_0 in place and B_y through the
+// separate tile.  Every wait has an iteration limit; a wait that runs out
+// sets stats->tma_err and the CTA returns.
+constexpr int TP_CW = 8;                           // compute warps = columns
+constexpr int TP_THREADS = 32 * (TP_CW + 1);
+constexpr int TP_BOX = 256;                        // rows per box
+
+// element (row, column c) of a swizzled 8-column tile, in complex units
+__device__ __forceinline__ int tix(int row, int c) {
+  return row * 8 + ((((c >> 1) ^ ((row >> 1) & 3)) << 1) | (c & 1));
+}
+
+template <int E>
+struct TpLayout {
+  static constexpr int n = 32 * E;
+  static constexpr size_t tile = (size_t) n * 64;  // bytes of one tile
+  // [twiddles n cplx][pad to 1 KB][stage 0: NIN tiles][stage 1][separate tile][scratch][barriers]
+  static constexpr size_t tw_bytes = ((size_t) n * 8 + 1023) / 1024 * 1024;
+  static size_t bytes(int nin) {
+    return tw_bytes + (2 * (size_t) nin + 1) * tile + (size_t) TP_CW * n * 8 + 64 + 1024;
+  }
+};
+
+template <int E, int PASS>
+__global__ void __maxnreg__(224)
+tpass_kernel(const __grid_constant__ CUtensorMap mi0, const __grid_constant__ CUtensorMap mi1,
+    const __grid_constant__ CUtensorMap mo0, const __grid_constant__ CUtensorMap mo1,
+    const __grid_constant__ CUtensorMap mo2, int Ng, int nkt, int ntiles,
+    const cplx *__restrict__ twn, EzCicStats *stats) {
+  typedef TpLayout<E> Lay;
+  constexpr int n = Lay::n;
+  constexpr int NIN = PASS == 0 ? 1 : 2;          // tiles loaded per stage
+  constexpr int NB = n / TP_BOX > 0 ? n / TP_BOX : 1;   // boxes per tile
+  constexpr int BR = n < TP_BOX ? n : TP_BOX;      // rows per box
+  extern __shared__ unsigned char tp_raw[];
+  // 1 KB alignment of every tile (the swizzle pattern repeats every 512 B)
+  unsigned char *base = (unsigned char *) (((uintptr_t) tp_raw + 1023) & ~(uintptr_t) 1023);
+  cplx *tw = (cplx *) base;
+  unsigned char *stg = base + Lay::tw_bytes;
+  cplx *sep = (cplx *) (stg + 2 * NIN * Lay::tile);
+  cplx *scr = (cplx *) ((unsigned char *) sep + Lay::tile);
+  uint64_t *bar = (uint64_t *) ((unsigned char *) scr + (size_t) TP_CW * n * 8);
+  uint64_t *full = bar, *empty = bar + 2, *sepfree = bar + 4;
+  auto in_tile = [&](int s, int a) { return (cplx *) (stg + ((size_t) s * NIN + a) * Lay::tile); };
+
+  for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
+  if (threadIdx.x == 0) {
+    ez_mbar_init(&full[0], 1);
+    ez_mbar_init(&full[1], 1);
+    ez_mbar_init(&empty[0], TP_CW);
+    ez_mbar_init(&empty[1], TP_CW);
+    ez_mbar_init(sepfree, 1);
+    ez_fence_mbar_init();
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int G = gridDim.x;
+
+  if (warp == TP_CW) {
+    // ---- producer ----
+    if (lane != 0) return;
+    ez_prefetch_map(&mi0);
+    if (NIN > 1) ez_prefetch_map(&mi1);
+    auto coords = [&](int t, int b, int &c0, int &c1, int &c2) {
+      const int o = t / nkt, kt = t - o * nkt;
+      c0 = 16 * kt;
+      if (PASS == 0) { c1 = o; c2 = b * BR; }      // tile: all i at j = o
+      else { c1 = b * BR; c2 = o; }                // tile: all j at i = o
+    };
+    int nload0 = 0, nload1 = 0;      // loads issued per stage
+    auto issue_load = [&](int it, int s) {
+      const int t = blockIdx.x + it * G;
+      if (s) nload1++; else nload0++;
+      ez_mbar_expect_tx(&full[s], (uint32_t) (NIN * Lay::tile));
+#pragma unroll
+      for (int a = 0; a < NIN; a++)
+        for (int b = 0; b < NB; b++) {
+          int c0, c1, c2;
+          coords(t, b, c0, c1, c2);
+          ez_tma_load3((unsigned char *) in_tile(s, a) + (size_t) b * BR * 64, a ? &mi1 : &mi0,
+              c0, c1, c2, &full[s]);
+        }
+    };
+    for (int it = 0; it < 2 && blockIdx.x + it * G < ntiles; it++) issue_load(it, it);
+    for (int it = 0; blockIdx.x + it * G < ntiles; it++) {
+      const int s = it & 1, t = blockIdx.x + it * G;
+      if (!ez_mbar_wait(&empty[s], (it >> 1) & 1)) {
+        // the compute warps gave up: let the copies in flight land first
+        atomicExch(&stats->tma_err, 1u);
+        if (nload0) ez_mbar_wait(&full[0], (nload0 - 1) & 1);
+        if (nload1) ez_mbar_wait(&full[1], (nload1 - 1) & 1);
+        break;
+      }
+      // stores of tile t.  Pass I: A_x (separate tile) -> mo0, A_0 (in
+      // place) -> mo1; pass J: B_x, B_0 (in place) -> mo0, mo1, B_y
+      // (separate tile) -> mo2
+      for (int b = 0; b < NB; b++) {
+        int c0, c1, c2;
+        coords(t, b, c0, c1, c2);
+        const size_t off = (size_t) b * BR * 64;
+        if (PASS == 0) {
+          ez_tma_store3(&mo0, c0, c1, c2, (const unsigned char *) sep + off);
+          ez_tma_store3(&mo1, c0, c1, c2, (const unsigned char *) in_tile(s, 0) + off);
+        } else {
+          ez_tma_store3(&mo0, c0, c1, c2, (const unsigned char *) in_tile(s, 0) + off);
+          ez_tma_store3(&mo1, c0, c1, c2, (const unsigned char *) in_tile(s, 1) + off);
+          ez_tma_store3(&mo2, c0, c1, c2, (const unsigned char *) sep + off);
+        }
+      }
+      ez_tma_commit();
+      ez_tma_wait_read<0>();         // the stage and the separate tile are free
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(ez_smem_addr(sepfree)) : "memory");
+      if (blockIdx.x + (it + 2) * G < ntiles) issue_load(it + 2, s);
+    }
+    ez_tma_wait_all();
+    return;
+  }
+
+  // ---- compute warps: column c = warp of every tile ----
+  const int c = warp;
+  cplx *line = scr + (size_t) warp * n;
+  auto col_load = [&](const cplx *tile, bool mulf, cplx *v) {
+#pragma unroll
+    for (int m = 0; m < E; m++) {
+      const int row = 32 * m + lane;
+      v[m] = tile[tix(row, c)];
+      if (mulf) {
+        const rt f = freq_of(row, Ng);
+        v[m].x *= f;
+        v[m].y *= f;
+      }
+    }
+  };
+  auto col_store = [&](cplx *tile, const cplx *v) {
+#pragma unroll
+    for (int q = 0; q < E; q++) tile[tix(W2<E>::out(lane, q), c)] = v[q];
+  };
+  for (int it = 0; blockIdx.x + it * G < ntiles; it++) {
+    const int s = it & 1;
+    if (!ez_mbar_wait(&full[s], (it >> 1) & 1)) { atomicExch(&stats->tma_err, 1u); return; }
+    cplx v[E];
+    if (PASS == 0) {
+      cplx *S = in_tile(s, 0);
+      if (it > 0 && !ez_mbar_wait(sepfree, (it - 1) & 1)) { atomicExch(&stats->tma_err, 1u); return; }
+      col_load(S, true, v);                        // A_x = FFT_i(S k_x)
+      warp_fft2<E, 1>(v, tw, lane, line);
+      col_store(sep, v);
+      col_load(S, false, v);                       // A_0 = FFT_i(S), in place
+      warp_fft2<E, 1>(v, tw, lane, line);
+      col_store(S, v);
+    } else {
+      cplx *Ax = in_tile(s, 0), *A0 = in_tile(s, 1);
+      col_load(Ax, false, v);                      // B_x = FFT_j(A_x), in place
+      warp_fft2<E, 1>(v, tw, lane, line);
+      col_store(Ax, v);
+      if (it > 0 && !ez_mbar_wait(sepfree, (it - 1) & 1)) { atomicExch(&stats->tma_err, 1u); return; }
+      col_load(A0, true, v);                       // B_y = FFT_j(A_0 k_y)
+      warp_fft2<E, 1>(v, tw, lane, line);
+      col_store(sep, v);
+      col_load(A0, false, v);                      // B_0 = FFT_j(A_0), in place
+      warp_fft2<E, 1>(v, tw, lane, line);
+      col_store(A0, v);
+    }
+    ez_fence_async_smem();
+    __syncwarp();
+    if (lane == 0)
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(ez_smem_addr(&empty[s])) : "memory");
   }
 }
 
@@ -602,10 +877,9 @@ wpass_k(const cplx *__restrict__ s0, const cplx *__restrict__ s1,
         v[m].x = er - oi;
         v[m].y = ei + orr;
       }
-      warp_fft<E, 1>(v, tw, lane);
-      const int r = brev5(lane);
+      line_fft<E, 1, use_t<E>(2)>(v, tw, lane, sl);
 #pragma unroll
-      for (int k = 0; k < E; k++) sl[swz(k + E * r)] = v[k];
+      for (int q = 0; q < E; q++) sl[swz(line_out<E, use_t<E>(2)>(lane, q))] = v[q];
       __syncwarp();
       cplx *d2 = (cplx *) dst;
 #pragma unroll
@@ -798,6 +1072,88 @@ bool warp_path(int Ng) {
   return sizeof(cplx) * ((size_t) Ng + 3 * WK * (size_t) (Ng + 1)) <= 227 * 1024;
 }
 
+}  // namespace
+
+bool ez_tma_encode(CUtensorMap *map, CUtensorMapDataType type, int rank, void *base,
+    const uint64_t *dims, const uint64_t *strides_bytes, const uint32_t *box,
+    CUtensorMapSwizzle swizzle) {
+  typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+      const cuuint64_t *, const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+      CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+      CUtensorMapFloatOOBfill);
+  static std::mutex mu;
+  static EncodeFn fn = nullptr;
+  static bool tried = false;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!tried) {
+      tried = true;
+      void *p = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      if (EZ_CUDA_OK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q)) &&
+          q == cudaDriverEntryPointSuccess)
+        fn = (EncodeFn) p;
+      else
+        cudaGetLastError();
+    }
+  }
+  if (!fn) return false;
+  cuuint64_t d[5], st[4];
+  cuuint32_t bx[5], es[5];
+  for (int i = 0; i < rank; i++) { d[i] = dims[i]; bx[i] = box[i]; es[i] = 1; }
+  for (int i = 0; i + 1 < rank; i++) st[i] = strides_bytes[i];
+  return fn(map, type, (cuuint32_t) rank, base, d, st, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+namespace {
+
+// Passes I and J through tpass_kernel (FP32, E = 8 or 16).  False if the
+// tensor maps cannot be made (then the cp.async kernels run instead).
+template <int E>
+bool run_tpass_ij(EzMesh *m, const FftPlanDev &pn) {
+  const int Ng = m->Ng;
+  if (sizeof(rt) != 4 || 32 * E != Ng) return false;
+  const uint64_t dims[3] = {2 * (uint64_t) m->Nkp, (uint64_t) Ng, (uint64_t) Ng};
+  const uint64_t str[2] = {2 * (uint64_t) m->Nkp * sizeof(rt),
+                           2 * (uint64_t) m->Nkp * Ng * sizeof(rt)};
+  const uint32_t br = (uint32_t) std::min(Ng, TP_BOX);
+  const uint32_t box_i[3] = {16, 1, br}, box_j[3] = {16, br, 1};
+  CUtensorMap mi[3], mj[3];
+  for (int a = 0; a < 3; a++)
+    if (!ez_tma_encode(&mi[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, m->spec[a], dims, str, box_i,
+                       CU_TENSOR_MAP_SWIZZLE_64B) ||
+        !ez_tma_encode(&mj[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, m->spec[a], dims, str, box_j,
+                       CU_TENSOR_MAP_SWIZZLE_64B))
+      return false;
+  const size_t smi = TpLayout<E>::bytes(1), smj = TpLayout<E>::bytes(2);
+  if (!EZ_CUDA_OK(cudaFuncSetAttribute(tpass_kernel<E, 0>,
+          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smi)) ||
+      !EZ_CUDA_OK(cudaFuncSetAttribute(tpass_kernel<E, 1>,
+          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smj))) {
+    cudaGetLastError();
+    return false;
+  }
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+  const int nkt = (m->Nk + WK - 1) / WK;
+  const int ntiles = Ng * nkt;
+  const unsigned grid = (unsigned) std::min(nsm, ntiles);
+  EzCicStats *stats = (EzCicStats *) m->stats;
+  ez_stage_begin(m, ST_FFT_I);
+  // pass I: S (spec0) -> A_x (spec1), A_0 (spec2)
+  tpass_kernel<E, 0><<<grid, TP_THREADS, smi, m->stream>>>(mi[0], mi[0], mi[1], mi[2], mi[2],
+      Ng, nkt, ntiles, pn.tw, stats); ez_count_launch();
+  ez_stage_end(m, ST_FFT_I);
+  ez_stage_begin(m, ST_FFT_J);
+  // pass J: A_x (spec1), A_0 (spec2) -> B_x (spec1), B_0 (spec2), B_y (spec0)
+  tpass_kernel<E, 1><<<grid, TP_THREADS, smj, m->stream>>>(mj[1], mj[2], mj[1], mj[2], mj[0],
+      Ng, nkt, ntiles, pn.tw, stats); ez_count_launch();
+  ez_stage_end(m, ST_FFT_J);
+  return true;
+}
+
 template <int E>
 int run_wpass_ij(EzMesh *m, const FftPlanDev &pn) {
   const int Ng = m->Ng;
@@ -844,12 +1200,20 @@ int ez_fft_c2r_psi(EzMesh *m) {
       return EZMOCK_ERR_UNKNOWN;
     const cplx *twg = twiddles(m->device, Ng);
     if (!twg) return EZMOCK_ERR_UNKNOWN;
-    switch (Ei) {
-      case 2: run_wpass_ij<2>(m, pn); break;
-      case 4: run_wpass_ij<4>(m, pn); break;
-      case 8: run_wpass_ij<8>(m, pn); break;
-      case 16: run_wpass_ij<16>(m, pn); break;
-      default: run_wpass_ij<32>(m, pn); break;
+    bool done = false;
+    cudaMemsetAsync(&((EzCicStats *) m->stats)->tma_err, 0, sizeof(unsigned int), m->stream);
+    if (m->fft_tma) {
+      if (Ei == 8) done = run_tpass_ij<8>(m, pn);
+      else if (Ei == 16) done = run_tpass_ij<16>(m, pn);
+    }
+    if (!done) {
+      switch (Ei) {
+        case 2: run_wpass_ij<2>(m, pn); break;
+        case 4: run_wpass_ij<4>(m, pn); break;
+        case 8: run_wpass_ij<8>(m, pn); break;
+        case 16: run_wpass_ij<16>(m, pn); break;
+        default: run_wpass_ij<32>(m, pn); break;
+      }
     }
     cudaMemsetAsync(&((EzCicStats *) m->stats)->psimax_bits, 0, sizeof(unsigned int), m->stream);
     switch (Ek) {

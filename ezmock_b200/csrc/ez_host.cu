@@ -414,6 +414,7 @@ EZMOCK *EZmock_init(const double Lbox, const int Ngrid, const int randgen,
   par->pdf_base = par->sigma_v = HUGE_VAL;
   EzMesh *m = MESH(ez);
   m->device = -1;
+  m->fft_tma = true;
   return ez;
 }
 
@@ -1015,6 +1016,10 @@ int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     case EZMOCKB200_OPT_CIC_TILE:
       if (value != 16 && value != 32) return (*err = EZMOCK_ERR_ARG_PARAMS);
       m->cic_legacy = value == 16;
+      return 0;
+    case EZMOCKB200_OPT_FFT_TMA:
+      if (value != 0 && value != 1) return (*err = EZMOCK_ERR_ARG_PARAMS);
+      m->fft_tma = value == 1;
       return 0;
     default: return (*err = EZMOCK_ERR_ARG_PARAMS);
   }

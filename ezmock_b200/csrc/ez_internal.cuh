@@ -85,7 +85,8 @@ struct EzMesh {
   int cic_mode;            // 0: float atomics, 1: deterministic fixed-point
   int cic_oh;              // halo of the owner-computes CIC (2; otherwise 3)
   bool cic_oh_set;         // cic_oh set by the caller for the next field
-  bool cic_legacy;         // FP32 CIC on 16 x 16 tiles instead of 32 x 32
+  bool cic_legacy;         // FP32 CIC on 16 x 16 tiles instead of 16 x 32
+  bool fft_tma;            // FP32 FFT passes I and J through TMA-staged tiles
 
   int Ng;
   size_t N;                // Ng^3
@@ -152,7 +153,7 @@ struct EzCicStats {
   unsigned int psimax_bits;   // max |psi| over the three fields (float bits)
   unsigned int nlist;         // far-displaced particles listed for fixup
   unsigned int nfar2;         // particles displaced by more than 2 cells on some axis
-  int pad;
+  unsigned int tma_err;       // a TMA-staged FFT pass gave up waiting (never expected)
 };
 
 // ---- error helpers ----

@@ -1367,9 +1367,12 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
       bscan, dbias, ran, (double) (real) EZ_GAUSS_WIDTH, hist); ez_count_launch();
   unsigned long long h[EZ_NLOGB], nvalid = 0;
+  unsigned int tma_err = 0;        // the field's TMA-staged FFT passes gave up
   if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaMemcpyAsync(&nvalid, bscan + nblk, 8, cudaMemcpyDeviceToHost, st)) ||
-      !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+      !EZ_CUDA_OK(cudaMemcpyAsync(&tma_err, &((EzCicStats *) m->stats)->tma_err, sizeof(tma_err),
+          cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaStreamSynchronize(st)) || tma_err)
     return EZMOCK_ERR_UNKNOWN;
   res->nvalid = nvalid;
   if (nvalid < ncell) { res->err = EZMOCK_ERR_RHO_LESS; return 0; }

@@ -18,7 +18,7 @@ bool ez_tma_encode(CUtensorMap *map, CUtensorMapDataType type, int rank, void *b
 
 // Iterations of an mbarrier wait before it gives up (a TMA copy lands within
 // microseconds; the limit only bounds a wait that would otherwise not end).
-#define EZ_TMA_SPIN_LIMIT (1u << 26)
+#define EZ_TMA_SPIN_LIMIT (1u << 22)
 
 __device__ __forceinline__ uint32_t ez_smem_addr(const void *p) {
   return (uint32_t) __cvta_generic_to_shared(p);

@@ -29,10 +29,14 @@ extern "C" {
    malloc() blocks for the next catalogues (a worker thread faults them in
    while the GPU computes); 0 turns the pool off.  Default 2048. */
 #define EZMOCKB200_OPT_HOST_POOL 6
-/* Column tile of the FP32 density assignment: 32 (32 x 32 cells, the
+/* Column tile of the FP32 density assignment: 32 (16 x 32 cells, the
    default, for grids that are multiples of 32) or 16 (16 x 16 cells).  Both
    give the same field. */
 #define EZMOCKB200_OPT_CIC_TILE 7
+/* FP32 transforms of the initial field along x and y: 1 (default) moves the
+   tiles with the Tensor Memory Accelerator on grids of 256^3 and 512^3, 0
+   with per-thread asynchronous copies.  Both give the same field. */
+#define EZMOCKB200_OPT_FFT_TMA 8
 
 int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     int *err);
