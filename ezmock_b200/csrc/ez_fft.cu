@@ -652,23 +652,27 @@ wpass_j(cplx *__restrict__ s0, cplx *__restrict__ s1, cplx *__restrict__ s2,
   }
 }
 
-// ------------------------------------------------ TMA-staged passes I, J --
+// ----------------------------------------------------- TMA-staged pass J --
 //
-// FP32, Ng = 32 E with E = 8 or 16.  The same transforms as wpass_i/j, with
-// tiles of WK = 8 columns moved by the Tensor Memory Accelerator: a tile is
-// Ng rows (i in pass I, j in pass J) of 64 bytes, copied by 256-row boxes of
-// a tensor map over the spectrum (floats, 2 Nkp x Ng x Ng) with the 64-byte
-// swizzle, so that a warp reading one column (one line) meets each bank at
-// most twice.  A persistent CTA per SM runs a two-stage pipeline: one
-// producer warp issues the loads of tile t + 2 and the stores of tile t from
-// shared memory, eight compute warps transform tile t + 1 (one column each,
-// the transposed line form warp_fft2 with a per-warp scratch line).  Pass I
-// reads S and writes A_0 in place of it and A_x through a separate tile;
-// pass J reads A_x and A_0, writes B_x and B_0 in place and B_y through the
-// separate tile.  Every wait has an iteration limit; a wait that runs out
-// sets stats->tma_err and the CTA returns.
-constexpr int TP_CW = 8;                           // compute warps = columns
-constexpr int TP_THREADS = 32 * (TP_CW + 1);
+// FP32, Ng = 32 E with E = 8 or 16.  The transforms of wpass_j, with tiles of
+// WK = 8 columns moved by the Tensor Memory Accelerator: a tile is Ng rows
+// (all j of one i) of 64 bytes, copied by 256-row boxes of a tensor map over
+// the spectrum (floats, 2 Nkp x Ng x Ng) with the 64-byte swizzle, so that a
+// warp reading one column (one line) meets each bank at most twice.  A
+// persistent CTA per SM runs a two-stage pipeline: while its eight warps
+// transform tile t (one column each, the transposed line form warp_fft2 with
+// a per-warp scratch line), the loads of tile t + 1 are in flight; thread 0
+// then stores tile t from shared memory and loads tile t + 2 into the
+// freed stage.  A_x and A_0 arrive; B_x and B_0 replace them in place and
+// B_y goes through a separate tile.  Every wait has an iteration limit; a
+// wait that runs out sets stats->tma_err (read by the population) and the
+// CTA lets its copies land and returns.  (Pass I through the same pipeline
+// measured slower than its cp.async kernel: 1.01 against 0.71 ms at 512^3;
+// it does two transforms per loaded tile, and one CTA of eight warps per SM,
+// which the 237 registers of the transforms allow, hides less latency than
+// the two CTAs of wpass_i.)
+constexpr int TP_CW = 8;                           // warps = columns of a tile
+constexpr int TP_THREADS = 32 * TP_CW;
 constexpr int TP_BOX = 256;                        // rows per box
 
 // element (row, column c) of a swizzled 8-column tile, in complex units
@@ -687,15 +691,15 @@ struct TpLayout {
   }
 };
 
-template <int E, int PASS>
-__global__ void __maxnreg__(224)
-tpass_kernel(const __grid_constant__ CUtensorMap mi0, const __grid_constant__ CUtensorMap mi1,
+template <int E>
+__global__ void __launch_bounds__(TP_THREADS, 1)
+tpass_j_kernel(const __grid_constant__ CUtensorMap mi0, const __grid_constant__ CUtensorMap mi1,
     const __grid_constant__ CUtensorMap mo0, const __grid_constant__ CUtensorMap mo1,
     const __grid_constant__ CUtensorMap mo2, int Ng, int nkt, int ntiles,
     const cplx *__restrict__ twn, EzCicStats *stats) {
   typedef TpLayout<E> Lay;
   constexpr int n = Lay::n;
-  constexpr int NIN = PASS == 0 ? 1 : 2;          // tiles loaded per stage
+  constexpr int NIN = 2;                           // A_x, A_0 per stage
   constexpr int NB = n / TP_BOX > 0 ? n / TP_BOX : 1;   // boxes per tile
   constexpr int BR = n < TP_BOX ? n : TP_BOX;      // rows per box
   extern __shared__ unsigned char tp_raw[];
@@ -708,81 +712,49 @@ tpass_kernel(const __grid_constant__ CUtensorMap mi0, const __grid_constant__ CU
   uint64_t *bar = (uint64_t *) ((unsigned char *) scr + (size_t) TP_CW * n * 8);
   uint64_t *full = bar, *empty = bar + 2, *sepfree = bar + 4;
   auto in_tile = [&](int s, int a) { return (cplx *) (stg + ((size_t) s * NIN + a) * Lay::tile); };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int G = gridDim.x;
+  const bool producer = threadIdx.x == 0;
+
+  auto coords = [&](int t, int b, int &c0, int &c1, int &c2) {
+    const int o = t / nkt, kt = t - o * nkt;
+    c0 = 16 * kt;                                  // tile: all j at i = o
+    c1 = b * BR;
+    c2 = o;
+  };
+  int nload0 = 0, nload1 = 0;                      // loads issued per stage
+  auto issue_load = [&](int it, int s) {
+    const int t = blockIdx.x + it * G;
+    if (s) nload1++; else nload0++;
+    ez_mbar_expect_tx(&full[s], (uint32_t) (NIN * Lay::tile));
+#pragma unroll
+    for (int a = 0; a < NIN; a++)
+#pragma unroll
+      for (int b = 0; b < NB; b++) {
+        int c0, c1, c2;
+        coords(t, b, c0, c1, c2);
+        ez_tma_load3((unsigned char *) in_tile(s, a) + (size_t) b * BR * 64, a ? &mi1 : &mi0,
+            c0, c1, c2, &full[s]);
+      }
+  };
 
   for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
-  if (threadIdx.x == 0) {
+  if (producer) {
     ez_mbar_init(&full[0], 1);
     ez_mbar_init(&full[1], 1);
     ez_mbar_init(&empty[0], TP_CW);
     ez_mbar_init(&empty[1], TP_CW);
     ez_mbar_init(sepfree, 1);
     ez_fence_mbar_init();
+    ez_prefetch_map(&mi0);
+    ez_prefetch_map(&mi1);
+    for (int it = 0; it < 2 && blockIdx.x + it * G < ntiles; it++) issue_load(it, it);
   }
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int G = gridDim.x;
 
-  if (warp == TP_CW) {
-    // ---- producer ----
-    if (lane != 0) return;
-    ez_prefetch_map(&mi0);
-    if (NIN > 1) ez_prefetch_map(&mi1);
-    auto coords = [&](int t, int b, int &c0, int &c1, int &c2) {
-      const int o = t / nkt, kt = t - o * nkt;
-      c0 = 16 * kt;
-      if (PASS == 0) { c1 = o; c2 = b * BR; }      // tile: all i at j = o
-      else { c1 = b * BR; c2 = o; }                // tile: all j at i = o
-    };
-    int nload0 = 0, nload1 = 0;      // loads issued per stage
-    auto issue_load = [&](int it, int s) {
-      const int t = blockIdx.x + it * G;
-      if (s) nload1++; else nload0++;
-      ez_mbar_expect_tx(&full[s], (uint32_t) (NIN * Lay::tile));
-#pragma unroll
-      for (int a = 0; a < NIN; a++)
-        for (int b = 0; b < NB; b++) {
-          int c0, c1, c2;
-          coords(t, b, c0, c1, c2);
-          ez_tma_load3((unsigned char *) in_tile(s, a) + (size_t) b * BR * 64, a ? &mi1 : &mi0,
-              c0, c1, c2, &full[s]);
-        }
-    };
-    for (int it = 0; it < 2 && blockIdx.x + it * G < ntiles; it++) issue_load(it, it);
-    for (int it = 0; blockIdx.x + it * G < ntiles; it++) {
-      const int s = it & 1, t = blockIdx.x + it * G;
-      if (!ez_mbar_wait(&empty[s], (it >> 1) & 1)) {
-        // the compute warps gave up: let the copies in flight land first
-        atomicExch(&stats->tma_err, 1u);
-        if (nload0) ez_mbar_wait(&full[0], (nload0 - 1) & 1);
-        if (nload1) ez_mbar_wait(&full[1], (nload1 - 1) & 1);
-        break;
-      }
-      // stores of tile t.  Pass I: A_x (separate tile) -> mo0, A_0 (in
-      // place) -> mo1; pass J: B_x, B_0 (in place) -> mo0, mo1, B_y
-      // (separate tile) -> mo2
-      for (int b = 0; b < NB; b++) {
-        int c0, c1, c2;
-        coords(t, b, c0, c1, c2);
-        const size_t off = (size_t) b * BR * 64;
-        if (PASS == 0) {
-          ez_tma_store3(&mo0, c0, c1, c2, (const unsigned char *) sep + off);
-          ez_tma_store3(&mo1, c0, c1, c2, (const unsigned char *) in_tile(s, 0) + off);
-        } else {
-          ez_tma_store3(&mo0, c0, c1, c2, (const unsigned char *) in_tile(s, 0) + off);
-          ez_tma_store3(&mo1, c0, c1, c2, (const unsigned char *) in_tile(s, 1) + off);
-          ez_tma_store3(&mo2, c0, c1, c2, (const unsigned char *) sep + off);
-        }
-      }
-      ez_tma_commit();
-      ez_tma_wait_read<0>();         // the stage and the separate tile are free
-      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(ez_smem_addr(sepfree)) : "memory");
-      if (blockIdx.x + (it + 2) * G < ntiles) issue_load(it + 2, s);
-    }
-    ez_tma_wait_all();
-    return;
-  }
-
-  // ---- compute warps: column c = warp of every tile ----
+  // every warp transforms column c = warp of each tile; thread 0 also issues
+  // the copies: after its warp's part of tile t it waits for the other
+  // warps, stores tile t, and loads tile t + 2 into the freed stage
   const int c = warp;
   cplx *line = scr + (size_t) warp * n;
   auto col_load = [&](const cplx *tile, bool mulf, cplx *v) {
@@ -801,36 +773,60 @@ tpass_kernel(const __grid_constant__ CUtensorMap mi0, const __grid_constant__ CU
 #pragma unroll
     for (int q = 0; q < E; q++) tile[tix(W2<E>::out(lane, q), c)] = v[q];
   };
-  for (int it = 0; blockIdx.x + it * G < ntiles; it++) {
-    const int s = it & 1;
-    if (!ez_mbar_wait(&full[s], (it >> 1) & 1)) { atomicExch(&stats->tma_err, 1u); return; }
+  bool ok = true;
+  for (int it = 0; ok && blockIdx.x + it * G < ntiles; it++) {
+    const int s = it & 1, t = blockIdx.x + it * G;
+    if (!ez_mbar_wait(&full[s], (it >> 1) & 1)) { atomicExch(&stats->tma_err, 1u); ok = false; }
     cplx v[E];
-    if (PASS == 0) {
-      cplx *S = in_tile(s, 0);
-      if (it > 0 && !ez_mbar_wait(sepfree, (it - 1) & 1)) { atomicExch(&stats->tma_err, 1u); return; }
-      col_load(S, true, v);                        // A_x = FFT_i(S k_x)
-      warp_fft2<E, 1>(v, tw, lane, line);
-      col_store(sep, v);
-      col_load(S, false, v);                       // A_0 = FFT_i(S), in place
-      warp_fft2<E, 1>(v, tw, lane, line);
-      col_store(S, v);
-    } else {
+    if (ok) {
       cplx *Ax = in_tile(s, 0), *A0 = in_tile(s, 1);
       col_load(Ax, false, v);                      // B_x = FFT_j(A_x), in place
       warp_fft2<E, 1>(v, tw, lane, line);
       col_store(Ax, v);
-      if (it > 0 && !ez_mbar_wait(sepfree, (it - 1) & 1)) { atomicExch(&stats->tma_err, 1u); return; }
-      col_load(A0, true, v);                       // B_y = FFT_j(A_0 k_y)
-      warp_fft2<E, 1>(v, tw, lane, line);
-      col_store(sep, v);
-      col_load(A0, false, v);                      // B_0 = FFT_j(A_0), in place
-      warp_fft2<E, 1>(v, tw, lane, line);
-      col_store(A0, v);
+      if (it > 0 && !ez_mbar_wait(sepfree, (it - 1) & 1)) { atomicExch(&stats->tma_err, 1u); ok = false; }
+      if (ok) {
+        col_load(A0, true, v);                     // B_y = FFT_j(A_0 k_y)
+        warp_fft2<E, 1>(v, tw, lane, line);
+        col_store(sep, v);
+        col_load(A0, false, v);                    // B_0 = FFT_j(A_0), in place
+        warp_fft2<E, 1>(v, tw, lane, line);
+        col_store(A0, v);
+      }
     }
     ez_fence_async_smem();
-    __syncwarp();
-    if (lane == 0)
+    ok = __all_sync(0xffffffffu, ok);              // (keeps a warp's lanes together)
+    if (ok && lane == 0)
       asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(ez_smem_addr(&empty[s])) : "memory");
+    if (producer && ok) {
+      if (!ez_mbar_wait(&empty[s], (it >> 1) & 1)) {
+        atomicExch(&stats->tma_err, 1u);
+        ok = false;
+      } else {
+        // stores of tile t: B_x, B_0 (in place) -> mo0, mo1, B_y (separate
+        // tile) -> mo2
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+          int c0, c1, c2;
+          coords(t, b, c0, c1, c2);
+          const size_t off = (size_t) b * BR * 64;
+          ez_tma_store3(&mo0, c0, c1, c2, (const unsigned char *) in_tile(s, 0) + off);
+          ez_tma_store3(&mo1, c0, c1, c2, (const unsigned char *) in_tile(s, 1) + off);
+          ez_tma_store3(&mo2, c0, c1, c2, (const unsigned char *) sep + off);
+        }
+        ez_tma_commit();
+        ez_tma_wait_read<0>();       // the stage and the separate tile are free
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(ez_smem_addr(sepfree)) : "memory");
+        if (blockIdx.x + (it + 2) * G < ntiles) issue_load(it + 2, s);
+      }
+    }
+    ok = __all_sync(0xffffffffu, ok);
+  }
+  if (producer) {
+    // copies in flight land before the CTA ends (an error path may leave
+    // loads unconsumed)
+    if (nload0) ez_mbar_wait(&full[0], (nload0 - 1) & 1);
+    if (nload1) ez_mbar_wait(&full[1], (nload1 - 1) & 1);
+    ez_tma_wait_all();
   }
 }
 
@@ -1109,28 +1105,23 @@ bool ez_tma_encode(CUtensorMap *map, CUtensorMapDataType type, int rank, void *b
 
 namespace {
 
-// Passes I and J through tpass_kernel (FP32, E = 8 or 16).  False if the
-// tensor maps cannot be made (then the cp.async kernels run instead).
+// Pass J through tpass_j_kernel (FP32, E = 8 or 16).  False if nothing was
+// launched (no tensor maps or a failed launch): the cp.async pass runs then.
 template <int E>
-bool run_tpass_ij(EzMesh *m, const FftPlanDev &pn) {
+bool run_tpass_j(EzMesh *m, const FftPlanDev &pn) {
   const int Ng = m->Ng;
   if (sizeof(rt) != 4 || 32 * E != Ng) return false;
   const uint64_t dims[3] = {2 * (uint64_t) m->Nkp, (uint64_t) Ng, (uint64_t) Ng};
   const uint64_t str[2] = {2 * (uint64_t) m->Nkp * sizeof(rt),
                            2 * (uint64_t) m->Nkp * Ng * sizeof(rt)};
-  const uint32_t br = (uint32_t) std::min(Ng, TP_BOX);
-  const uint32_t box_i[3] = {16, 1, br}, box_j[3] = {16, br, 1};
-  CUtensorMap mi[3], mj[3];
+  const uint32_t box[3] = {16, (uint32_t) std::min(Ng, TP_BOX), 1};
+  CUtensorMap mj[3];
   for (int a = 0; a < 3; a++)
-    if (!ez_tma_encode(&mi[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, m->spec[a], dims, str, box_i,
-                       CU_TENSOR_MAP_SWIZZLE_64B) ||
-        !ez_tma_encode(&mj[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, m->spec[a], dims, str, box_j,
+    if (!ez_tma_encode(&mj[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, m->spec[a], dims, str, box,
                        CU_TENSOR_MAP_SWIZZLE_64B))
       return false;
-  const size_t smi = TpLayout<E>::bytes(1), smj = TpLayout<E>::bytes(2);
-  if (!EZ_CUDA_OK(cudaFuncSetAttribute(tpass_kernel<E, 0>,
-          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smi)) ||
-      !EZ_CUDA_OK(cudaFuncSetAttribute(tpass_kernel<E, 1>,
+  const size_t smj = TpLayout<E>::bytes(2);
+  if (!EZ_CUDA_OK(cudaFuncSetAttribute(tpass_j_kernel<E>,
           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smj))) {
     cudaGetLastError();
     return false;
@@ -1140,38 +1131,49 @@ bool run_tpass_ij(EzMesh *m, const FftPlanDev &pn) {
   const int nkt = (m->Nk + WK - 1) / WK;
   const int ntiles = Ng * nkt;
   const unsigned grid = (unsigned) std::min(nsm, ntiles);
-  EzCicStats *stats = (EzCicStats *) m->stats;
-  ez_stage_begin(m, ST_FFT_I);
-  // pass I: S (spec0) -> A_x (spec1), A_0 (spec2)
-  tpass_kernel<E, 0><<<grid, TP_THREADS, smi, m->stream>>>(mi[0], mi[0], mi[1], mi[2], mi[2],
-      Ng, nkt, ntiles, pn.tw, stats); ez_count_launch();
-  ez_stage_end(m, ST_FFT_I);
   ez_stage_begin(m, ST_FFT_J);
-  // pass J: A_x (spec1), A_0 (spec2) -> B_x (spec1), B_0 (spec2), B_y (spec0)
-  tpass_kernel<E, 1><<<grid, TP_THREADS, smj, m->stream>>>(mj[1], mj[2], mj[1], mj[2], mj[0],
-      Ng, nkt, ntiles, pn.tw, stats); ez_count_launch();
+  // A_x (spec1), A_0 (spec2) -> B_x (spec1), B_0 (spec2), B_y (spec0)
+  tpass_j_kernel<E><<<grid, TP_THREADS, smj, m->stream>>>(mj[1], mj[2], mj[1], mj[2], mj[0],
+      Ng, nkt, ntiles, pn.tw, (EzCicStats *) m->stats); ez_count_launch();
   ez_stage_end(m, ST_FFT_J);
-  return true;
+  return EZ_CUDA_OK(cudaGetLastError());
 }
 
 template <int E>
-int run_wpass_ij(EzMesh *m, const FftPlanDev &pn) {
+int run_wpass_i(EzMesh *m, const FftPlanDev &pn) {
   const int Ng = m->Ng;
   const size_t n = 32 * E, LS = n + 1;
   const size_t sm_i = sizeof(cplx) * (n + 2 * WK * LS);
-  const size_t sm_j = sizeof(cplx) * (n + 3 * WK * LS);
   cudaFuncSetAttribute(wpass_i<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_i);
-  cudaFuncSetAttribute(wpass_j<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_j);
   const int nkt = (m->Nk + WK - 1) / WK;
   ez_stage_begin(m, ST_FFT_I);
   wpass_i<E><<<dim3(nkt, Ng), 32 * WNW, sm_i, m->stream>>>(m->spec[0], m->spec[1],
       m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
   ez_stage_end(m, ST_FFT_I);
+  return 0;
+}
+
+template <int E>
+int run_wpass_j(EzMesh *m, const FftPlanDev &pn) {
+  const int Ng = m->Ng;
+  const size_t n = 32 * E, LS = n + 1;
+  const size_t sm_j = sizeof(cplx) * (n + 3 * WK * LS);
+  cudaFuncSetAttribute(wpass_j<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_j);
+  const int nkt = (m->Nk + WK - 1) / WK;
   ez_stage_begin(m, ST_FFT_J);
   wpass_j<E><<<dim3(nkt, Ng), 32 * WNW, sm_j, m->stream>>>(m->spec[0], m->spec[1],
       m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
   ez_stage_end(m, ST_FFT_J);
   return 0;
+}
+
+template <int E>
+int run_wpass_ij(EzMesh *m, const FftPlanDev &pn) {
+  run_wpass_i<E>(m, pn);
+  if constexpr (E == 8 || E == 16) {
+    if (m->fft_tma && run_tpass_j<E>(m, pn)) return 0;
+  }
+  return run_wpass_j<E>(m, pn);
 }
 
 template <int E>
@@ -1200,20 +1202,13 @@ int ez_fft_c2r_psi(EzMesh *m) {
       return EZMOCK_ERR_UNKNOWN;
     const cplx *twg = twiddles(m->device, Ng);
     if (!twg) return EZMOCK_ERR_UNKNOWN;
-    bool done = false;
     cudaMemsetAsync(&((EzCicStats *) m->stats)->tma_err, 0, sizeof(unsigned int), m->stream);
-    if (m->fft_tma) {
-      if (Ei == 8) done = run_tpass_ij<8>(m, pn);
-      else if (Ei == 16) done = run_tpass_ij<16>(m, pn);
-    }
-    if (!done) {
-      switch (Ei) {
-        case 2: run_wpass_ij<2>(m, pn); break;
-        case 4: run_wpass_ij<4>(m, pn); break;
-        case 8: run_wpass_ij<8>(m, pn); break;
-        case 16: run_wpass_ij<16>(m, pn); break;
-        default: run_wpass_ij<32>(m, pn); break;
-      }
+    switch (Ei) {
+      case 2: run_wpass_ij<2>(m, pn); break;
+      case 4: run_wpass_ij<4>(m, pn); break;
+      case 8: run_wpass_ij<8>(m, pn); break;
+      case 16: run_wpass_ij<16>(m, pn); break;
+      default: run_wpass_ij<32>(m, pn); break;
     }
     cudaMemsetAsync(&((EzCicStats *) m->stats)->psimax_bits, 0, sizeof(unsigned int), m->stream);
     switch (Ek) {

@@ -16,7 +16,12 @@ extern "C" {
 #endif
 
 /* Options for EZmockB200_set_option. */
-#define EZMOCKB200_OPT_CIC_MODE 1   /* 0: float atomics (default), 1: deterministic */
+/* 0: the default assignment; 1: deterministic, bit-identical between runs
+   (64-bit fixed point, 2^-50 units for the density and 2^-40 for the painted
+   displacements, added with integer atomics): exact while no cell's density
+   reaches 8192 and no cell's summed displacement reaches 2^23 Mpc/h, far
+   above what a Zel'dovich field produces; beyond that the sums wrap. */
+#define EZMOCKB200_OPT_CIC_MODE 1
 #define EZMOCKB200_OPT_TIMING   2   /* 1: record per-stage CUDA-event timings */
 #define EZMOCKB200_OPT_DEVICE   3   /* CUDA device ordinal (before the first field) */
 #define EZMOCKB200_OPT_SEED     4   /* new random seed (> 0) for the next field */
@@ -91,7 +96,9 @@ int EZmockB200_rng_raw(const int randgen, const uint64_t seed,
    (built once per process), the device addresses of the static arrays, a
    copy of the 159,744-byte jump table; make that first call before any
    stream capture.  Later calls only launch kernels on `stream` and return
-   without waiting.  There is one scratch per device: calls that overlap on
+   without waiting.  The set-up is kept for the life of the process: a
+   device reset (cudaDeviceReset) while the library is loaded is not
+   supported, since the static arrays would come back zeroed.  There is one scratch per device: calls that overlap on
    the same device race on it, so the caller serialises them (one stream,
    one host thread at a time). */
 #define EZMOCKB200_NOALLOC_MAX_DRAWS ((uint64_t) 1 << 47)
