@@ -190,6 +190,29 @@ def test_cic_tiles_agree(pk_table, Ng, L):
     assert relmax(out[1][0], rho) <= 1e-5
 
 
+@pytest.mark.parametrize("Ng,L", [(256, 1250.0), (512, 2500.0)])
+def test_fft_tma_matches_cp_async(pk_table, Ng, L):
+    """The FP32 transforms along y staged by the Tensor Memory Accelerator
+    (the default on 256^3 and 512^3) and by per-thread cp.async copies give
+    the same displacement fields to single-precision rounding (their line
+    transforms differ in the order of the 32-point stages), and the TMA
+    fields are within the stated FP32 error of the FP64 oracle."""
+    k, P = pk_table
+    out = []
+    for tma in (1, 0):
+        m = make(32, Ng, L, 1, 9, k, P)
+        m.set_option(8, tma)
+        m.create_dens_field_from_ic()
+        out.append([m.field(d) for d in range(3)])
+        del m
+    for a, b in zip(*out):
+        assert relmax(a, b) <= 1e-6
+    if Ng == 256:
+        O, t, vf, psi, rho = oracle_field(64, Ng, L, 1, 9, k, P)
+        for d in range(3):
+            assert relmax(out[0][d], psi[d]) <= 5e-6
+
+
 @pytest.mark.parametrize("rng", [0, 1])
 def test_golden_reference_fp64(golden, pk_table, rng):
     """16^3 fields, counts and catalogue of the reference's own build."""
