@@ -178,6 +178,11 @@ class EZmock:
                                                         ctypes.byref(self._err))
         self._assert_return_value()
 
+    def select_path(self):
+        """How the last selection found its boundaries: 0 value buckets, 1 full
+        sort, 2 buckets then full sort."""
+        return int(self._L.EZmockB200_select_path(self._ez))
+
     def field(self, which):
         """Copy of a device field: 0..2 psi, 3 rho, 4..6 painted displacements."""
         out = np.empty(self._Ng ** 3, self._rdt)

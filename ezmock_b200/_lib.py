@@ -95,6 +95,8 @@ def load(prec=32):
     L.EZmockB200_real_size.argtypes = []
     L.EZmockB200_launch_count.restype = ctypes.c_longlong
     L.EZmockB200_launch_count.argtypes = []
+    L.EZmockB200_select_path.restype = ctypes.c_int
+    L.EZmockB200_select_path.argtypes = [ctypes.c_void_p]
     L.EZmockB200_mark.restype = ctypes.c_int
     L.EZmockB200_mark.argtypes = [_vp, ctypes.c_int]
     L.EZmockB200_elapsed.restype = ctypes.c_int

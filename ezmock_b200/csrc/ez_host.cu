@@ -415,6 +415,7 @@ EZMOCK *EZmock_init(const double Lbox, const int Ngrid, const int randgen,
   EzMesh *m = MESH(ez);
   m->device = -1;
   m->fft_tma = true;
+  m->sel_path = -1;
   return ez;
 }
 
@@ -1021,6 +1022,10 @@ int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
       if (value != 0 && value != 1) return (*err = EZMOCK_ERR_ARG_PARAMS);
       m->fft_tma = value == 1;
       return 0;
+    case EZMOCKB200_OPT_SELECT_SORT:
+      if (value != 0 && value != 1) return (*err = EZMOCK_ERR_ARG_PARAMS);
+      m->sel_sort = value == 1;
+      return 0;
     default: return (*err = EZMOCK_ERR_ARG_PARAMS);
   }
 }
@@ -1195,6 +1200,8 @@ int EZmockB200_sync(EZMOCK *ez) {
 int EZmockB200_real_size(void) { return (int) sizeof(real); }
 
 long long EZmockB200_launch_count(void) { return g_launches.load(); }
+
+int EZmockB200_select_path(EZMOCK *ez) { return ez ? MESH(ez)->sel_path : -1; }
 
 int EZmockB200_mark(EZMOCK *ez, const int slot) {
   if (!ez || slot < 0 || slot >= 8) return EZMOCK_ERR_ARG_PARAMS;

@@ -22,6 +22,7 @@
 #include "ez_internal.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 namespace {
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(NT)
 bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
     real thres, double iexp, const unsigned long long *off,
     const uint32_t *__restrict__ draws, int ran, double lambda,
-    unsigned long long *hist) {
+    unsigned long long *hist, uint16_t *chist) {
   constexpr int NW = NT / 32;
   __shared__ unsigned int pre[ROWS * NW];    // valid counts, then prefixes
   __shared__ unsigned int wsum[ROWS * NW / 32];
@@ -246,24 +247,56 @@ bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     if (id < N) rhot[id] = st[q * NT + threadIdx.x];
   }
-  if (threadIdx.x < EZ_NLOGB && sh[threadIdx.x])
-    atomicAdd(hist + threadIdx.x, (unsigned long long) sh[threadIdx.x]);
+  if (threadIdx.x < EZ_NLOGB) {
+    // the chunk's histogram, for the compaction's early reservation
+    chist[(size_t) blockIdx.x * EZ_NLOGB + threadIdx.x] = (uint16_t) sh[threadIdx.x];
+    if (sh[threadIdx.x]) atomicAdd(hist + threadIdx.x, (unsigned long long) sh[threadIdx.x]);
+  }
 }
 
 // Candidates (rho_t >= cut) of a 4096-cell chunk are counted, one atomic per
 // block reserves their slots, and their keys are written (the order of the
-// candidate list is irrelevant: it is sorted next).
+// candidate list is irrelevant: it is sorted next).  With the chunk
+// histograms of the bias stage (chist; cut = 2^(5 - imax) above the last
+// bin, so the candidates are the cells of bins 0..imax) the reservation is
+// made while the chunk's values are still being loaded, and the ballot count
+// is checked against it (counter[1] flags a difference).
+// Value buckets of the candidates for the boundary search below: a monotone
+// map of a candidate's bits (v >= cut > 0, so its bits order as its value),
+// SEL_NB buckets from the cut up; larger values share the last bucket.
+constexpr int SEL_NB = 32768;
+
+#ifdef SINGLE_PREC
+typedef uint32_t ubits_t;
+__device__ __forceinline__ ubits_t val_bits(real v) { return __float_as_uint(v); }
+#else
+typedef unsigned long long ubits_t;
+__device__ __forceinline__ ubits_t val_bits(real v) { return (ubits_t) __double_as_longlong(v); }
+#endif
+
+struct SelBucket {
+  ubits_t base;              // bits of the cut
+  int shift;
+};
+
+__device__ __forceinline__ int sel_bucket(real v, SelBucket sb) {
+  const ubits_t d = (val_bits(v) - sb.base) >> sb.shift;
+  return d < (ubits_t) SEL_NB ? (int) d : SEL_NB - 1;
+}
+
 __global__ void __launch_bounds__(NT)
 compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
     skey_t *__restrict__ keys, unsigned long long *counter, skey_t *__restrict__ cand,
     uint16_t *__restrict__ cidx, size_t ccap, unsigned long long *__restrict__ cstart,
-    unsigned int *__restrict__ ccnt) {
+    unsigned int *__restrict__ ccnt, unsigned int *bhist, SelBucket sb,
+    const uint16_t *__restrict__ chist, int imax) {
   // candidates are written warp row by warp row (ballot ranks), so each
   // warp's stores are contiguous; their order within the chunk's range is
   // irrelevant (the keys are sorted, the copies carry their place)
   constexpr int NW = NT / 32;
   __shared__ unsigned int wtot[NW];
-  __shared__ unsigned long long sbase;
+  __shared__ unsigned long long sbase, sres;
+  __shared__ bool sok;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const size_t b0 = (size_t) blockIdx.x * CH;
   real v[ROWS];
@@ -273,6 +306,16 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
   for (int q = 0; q < ROWS; q++) {               // all loads first
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     v[q] = (id < N) ? rhot[id] : (real) 0;
+  }
+  if (chist && w == 0) {                         // reservation while the loads fly
+    const uint16_t *hc = chist + (size_t) blockIdx.x * EZ_NLOGB;
+    unsigned int c = ((lane <= imax) ? hc[lane] : 0u) + ((lane + 32 <= imax) ? hc[lane + 32] : 0u);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) {
+      sres = c;
+      sbase = c ? atomicAdd(counter, (unsigned long long) c) : 0;
+    }
   }
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
@@ -285,11 +328,18 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
   if (threadIdx.x == 0) {
     unsigned long long tot = 0;
     for (int k = 0; k < NW; k++) tot += wtot[k];
-    sbase = tot ? atomicAdd(counter, tot) : 0;
+    sok = true;
+    if (!chist) sbase = tot ? atomicAdd(counter, tot) : 0;
+    else if (tot != sres) {
+      atomicAdd(counter + 1, 1ull);            // writes nothing; the stage fails
+      sok = false;
+      tot = 0;
+    }
     cstart[blockIdx.x] = sbase;
     ccnt[blockIdx.x] = (unsigned int) tot;
   }
   __syncthreads();
+  if (!sok) return;
   unsigned long long off = sbase;
   for (int k = 0; k < w; k++) off += wtot[k];
   const unsigned int lt = (1u << lane) - 1;
@@ -301,6 +351,7 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
       keys[pos] = k;
       // a second copy with the cell's place in the chunk, kept for emission
       if (pos < ccap) { cand[pos] = k; cidx[pos] = (uint16_t) (q * NT + threadIdx.x); }
+      if (bhist) atomicAdd(bhist + sel_bucket(v[q], sb), 1u);
     }
     off += __popc(bal[q]);
   }
@@ -477,6 +528,189 @@ __global__ void bounds_kernel(const skey_t *__restrict__ keys, size_t M,
   o->nbins = nb;
   o->ncell = ncell;
   o->ntot = ntot;
+}
+
+// ---- boundaries of the PDF bins from the value buckets ----
+//
+// Bin j ends at rank E_j = P_j + pdf[j] (ranks in descending value order)
+// and the next starts at E2_j, the rank after the ties of rank E_j - 1.  A
+// run of equal values lies in one bucket, so E2_j is at most the end of the
+// bucket holding rank E_j - 1.  sel_plan_kernel follows the chain with these
+// bounds (P_j in [Plo, Phi]) and marks every bucket that can hold rank
+// E_j - 1 for some admissible P_j; sel_gather_kernel copies the candidates of
+// the marked buckets (a few thousand of millions); sel_resolve_kernel sorts
+// them and runs bounds_kernel's exact chain on their ranks.  Results equal
+// bounds_kernel's on the fully sorted keys; when the marked buckets hold more
+// than SEL_GCAP candidates, sel_resolve_kernel asks for the full sort.
+constexpr int SEL_NT = 1024;
+constexpr int SEL_GCAP = 65536 / (int) sizeof(skey_t);   // gathered keys (64 KB)
+constexpr int SEL_FALLBACK = -2;                          // BoundOut.err: sort all
+constexpr size_t SEL_PLAN_SMEM = SEL_NB * sizeof(unsigned int);
+constexpr size_t SEL_RESOLVE_SMEM = SEL_PLAN_SMEM + SEL_GCAP * sizeof(skey_t);
+
+// cum[b] = candidates in buckets above b (exclusive prefix in descending
+// bucket order); returns the total.  All threads; ends with a barrier.
+__device__ unsigned int sel_cum(const unsigned int *__restrict__ bh, unsigned int *cum,
+    unsigned int *sw) {
+  constexpr int PER = SEL_NB / SEL_NT;
+  unsigned int c[PER], s = 0;
+#pragma unroll
+  for (int i = 0; i < PER; i++) {
+    c[i] = bh[SEL_NB - 1 - (threadIdx.x * PER + i)];
+    s += c[i];
+  }
+  unsigned int tot;
+  unsigned int run = block_scan<unsigned int>(s, &tot, sw);
+#pragma unroll
+  for (int i = 0; i < PER; i++) {
+    cum[SEL_NB - 1 - (threadIdx.x * PER + i)] = run;
+    run += c[i];
+  }
+  __syncthreads();
+  return tot;
+}
+
+// Bucket of rank r: the lowest b with cum[b] <= r (cum does not increase
+// with b; that b is non-empty).
+__device__ __forceinline__ int sel_rank_bucket(const unsigned int *cum, unsigned long long r) {
+  int lo = 0, hi = SEL_NB - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (cum[mid] <= r) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ unsigned long long sel_bucket_end(const unsigned int *cum, int b,
+    unsigned long long M) {
+  return b > 0 ? cum[b - 1] : M;
+}
+
+__global__ void __launch_bounds__(SEL_NT)
+sel_plan_kernel(const unsigned int *__restrict__ bh, unsigned long long M,
+    const unsigned long long *__restrict__ pdf, int nmax, unsigned int *mask_out) {
+  extern __shared__ unsigned int cum[];             // SEL_NB
+  __shared__ unsigned int sw[32];
+  __shared__ unsigned int mask[SEL_NB / 32];
+  for (int w = threadIdx.x; w < SEL_NB / 32; w += SEL_NT) mask[w] = 0;
+  sel_cum(bh, cum, sw);
+  if (threadIdx.x == 0) {
+    unsigned long long plo = 0, phi = 0;
+    for (int j = 0; j < nmax; j++) {
+      const unsigned long long q = pdf[j];
+      if (!q) continue;
+      const unsigned long long elo = plo + q;
+      if (elo > M) break;                            // the exact chain fails here
+      const unsigned long long ehi = min(phi + q, M);
+      const int bhi = sel_rank_bucket(cum, elo - 1);  // higher values, higher bucket
+      const int blo = sel_rank_bucket(cum, ehi - 1);
+      for (int w = blo >> 5; w <= (bhi >> 5); w++) {
+        const int a = max(blo - 32 * w, 0), b = min(bhi - 32 * w, 31);
+        mask[w] |= (b == 31 ? 0xffffffffu : ((2u << b) - 1)) & ~((1u << a) - 1);
+      }
+      plo = elo;
+      phi = sel_bucket_end(cum, blo, M);
+    }
+  }
+  __syncthreads();
+  for (int w = threadIdx.x; w < SEL_NB / 32; w += SEL_NT) mask_out[w] = mask[w];
+}
+
+__global__ void __launch_bounds__(NT)
+sel_gather_kernel(const skey_t *__restrict__ keys, size_t M, SelBucket sb,
+    const unsigned int *__restrict__ mask_g, unsigned int *gcount, skey_t *gbuf) {
+  __shared__ unsigned int mask[SEL_NB / 32];
+  for (int w = threadIdx.x; w < SEL_NB / 32; w += NT) mask[w] = mask_g[w];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const size_t stride = (size_t) gridDim.x * NT;
+  for (size_t b0 = (size_t) blockIdx.x * NT; b0 < M; b0 += stride) {   // block-uniform trips
+    const size_t i = b0 + threadIdx.x;
+    skey_t k = 0;
+    bool take = false;
+    if (i < M) {
+      k = keys[i];
+      const int b = sel_bucket(from_key(k), sb);
+      take = (mask[b >> 5] >> (b & 31)) & 1u;
+    }
+    const unsigned int bal = __ballot_sync(0xffffffffu, take);
+    if (bal) {
+      unsigned int p0 = 0;
+      if (lane == 0) p0 = atomicAdd(gcount, (unsigned int) __popc(bal));
+      p0 = __shfl_sync(0xffffffffu, p0, 0);
+      const unsigned int p = p0 + __popc(bal & ((1u << lane) - 1));
+      if (take && p < (unsigned int) SEL_GCAP) gbuf[p] = k;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SEL_NT)
+sel_resolve_kernel(const unsigned int *__restrict__ bh, unsigned long long M, SelBucket sb,
+    const unsigned int *__restrict__ gcount, const skey_t *__restrict__ gbuf,
+    const unsigned long long *__restrict__ pdf, int nmax, unsigned long long ncell,
+    unsigned long long ntot, BoundOut *o) {
+  extern __shared__ unsigned int cum[];             // SEL_NB, then the keys
+  skey_t *g = reinterpret_cast<skey_t *>(cum + SEL_NB);
+  __shared__ unsigned int sw[32];
+  const unsigned int tot = sel_cum(bh, cum, sw);
+  const unsigned int G = *gcount;
+  if (tot != M || G > (unsigned int) SEL_GCAP) {     // uniform over the block
+    if (threadIdx.x == 0) o->err = SEL_FALLBACK;
+    return;
+  }
+  int n2 = 1;
+  while (n2 < (int) G) n2 <<= 1;
+  for (int i = threadIdx.x; i < n2; i += SEL_NT) g[i] = (i < (int) G) ? gbuf[i] : ~(skey_t) 0;
+  __syncthreads();
+  // bitonic sort, ascending keys (descending values)
+  for (int k = 2; k <= n2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < n2; i += SEL_NT) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const skey_t a = g[i], b = g[ixj];
+          if ((a > b) == ((i & k) == 0)) { g[i] = b; g[ixj] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  if (threadIdx.x) return;
+  // bounds_kernel's chain; the key of rank r is found in the sorted gathered
+  // keys: its bucket b's keys start at the first key with bucket <= b
+  unsigned long long P = 0;
+  int nb = 0;
+  for (int j = 0; j < nmax; j++) {
+    unsigned long long q = pdf[j];
+    if (!q) { o->pdf[j] = 0; continue; }
+    unsigned long long E = P + q;
+    if (E > M) { o->err = EZMOCK_ERR_UNKNOWN; return; }
+    const int b = sel_rank_bucket(cum, E - 1);
+    int lo = 0, hi = (int) G;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (sel_bucket(from_key(g[mid]), sb) <= b) hi = mid; else lo = mid + 1;
+    }
+    const unsigned long long i = lo + (E - 1 - cum[b]);
+    if (i >= G || sel_bucket(from_key(g[i]), sb) != b) { o->err = SEL_FALLBACK; return; }
+    const skey_t kv = g[i];
+    unsigned long long ie = i;
+    while (ie + 1 < G && g[ie + 1] == kv) ie++;
+    const unsigned long long E2 = cum[b] + (ie - lo) + 1;
+    const unsigned long long extra = E2 - E;
+    q += extra;
+    ncell += extra;
+    ntot += extra * (unsigned long long) (nmax - j);
+    E = E2;
+    o->pdf[j] = q;
+    o->lo[nb] = from_key(kv);
+    o->ntr[nb] = nmax - j;
+    nb++;
+    P = E;
+  }
+  o->nbins = nb;
+  o->ncell = ncell;
+  o->ntot = ntot;
+  o->err = 0;
 }
 
 __device__ __forceinline__ int cell_count(real v, const real *lo, const int *ntr,
@@ -1170,6 +1404,11 @@ struct PopScratch {
   BoundOut *bo;
   unsigned long long *cstart;   // per chunk: first candidate (compact_kernel)
   unsigned int *ccnt;           // per chunk: candidates
+  unsigned int *bhist;          // SEL_NB candidate counts per value bucket
+  unsigned int *bmask;          // SEL_NB bits: buckets that can hold a boundary
+  unsigned int *gcount;         // candidates of the marked buckets
+  skey_t *gbuf;                 // their keys (SEL_GCAP)
+  uint16_t *chist;              // per chunk: log2 histogram of rho_t (bias stage)
 };
 
 // Candidate copies for emission, in the draws buffer (free between the bias
@@ -1206,7 +1445,12 @@ int pop_scratch(EzMesh *m, PopScratch *ps) {
   const size_t ntmp = (256 * ntile_max + nblk) / SCAN_CHUNK + 8;
   const size_t off_cst = off_tmp + ntmp * 8;
   const size_t off_ccn = off_cst + nblk * 8;
-  int e = ez_scratch(m, off_ccn + nblk * 4);
+  const size_t off_bh = (off_ccn + nblk * 4 + 255) / 256 * 256;
+  const size_t off_bm = off_bh + SEL_NB * 4;
+  const size_t off_gc = off_bm + SEL_NB / 8;
+  const size_t off_gb = off_gc + 256;
+  const size_t off_ch = (off_gb + SEL_GCAP * sizeof(skey_t) + 255) / 256 * 256;
+  int e = ez_scratch(m, off_ch + nblk * EZ_NLOGB * sizeof(uint16_t));
   if (e) return e;
   char *sc = (char *) m->scratch;
   ps->bcnt = (unsigned long long *) (sc + off_cnt);
@@ -1220,6 +1464,11 @@ int pop_scratch(EzMesh *m, PopScratch *ps) {
   ps->tmp = (unsigned long long *) (sc + off_tmp);
   ps->cstart = (unsigned long long *) (sc + off_cst);
   ps->ccnt = (unsigned int *) (sc + off_ccn);
+  ps->bhist = (unsigned int *) (sc + off_bh);
+  ps->bmask = (unsigned int *) (sc + off_bm);
+  ps->gcount = (unsigned int *) (sc + off_gc);
+  ps->gbuf = (skey_t *) (sc + off_gb);
+  ps->chist = (uint16_t *) (sc + off_ch);
   return 0;
 }
 
@@ -1229,55 +1478,81 @@ struct HostBounds {
   int nbins;
 };
 
+// Full LSD radix sort of the M candidate keys in keys_a (keys_b: scratch);
+// returns the sorted copy.
+skey_t *sort_keys(const PopScratch &ps, skey_t *keys_a, skey_t *keys_b, size_t M,
+    cudaStream_t st) {
+  if (M <= 1) return keys_a;
+  const size_t ntiles = (M + TILE - 1) / TILE;
+  skey_t *src = keys_a, *dst = keys_b;
+  for (int shift = 0; shift < (int) (8 * sizeof(skey_t)); shift += 8) {
+    digit_hist_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, M, shift, ps.dcount, ntiles); ez_count_launch();
+    scan_u64(ps.dcount, ps.dcscan, 256 * ntiles, ps.tmp, st);
+    digit_scatter_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, dst, M, shift, ps.dcscan, ntiles); ez_count_launch();
+    skey_t *t = src; src = dst; dst = t;
+  }
+  return src;
+}
+
+ubits_t host_bits(real v) {
+  ubits_t b;
+  memcpy(&b, &v, sizeof(b));
+  return b;
+}
+
 // Selection (pop_tracer.c:359-461): cut from the log2 histogram, compaction
-// of the candidates, radix sort of their keys, PDF-bin boundaries with the
-// tie extension.  Leaves the boundaries in ps.bo on the device.
+// of the candidates, PDF-bin boundaries with the tie extension (from the
+// value buckets, or from a full sort).  Leaves the boundaries in ps.bo on
+// the device.
 int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
     const unsigned long long *h, const size_t *pdf, int nmax, size_t ncell,
-    size_t ntot, HostBounds *hb, CandBuf *cb = nullptr) {
+    size_t ntot, HostBounds *hb, CandBuf *cb = nullptr, const uint16_t *chist = nullptr) {
   const size_t N = m->N;
   cudaStream_t st = m->stream;
   skey_t *keys_a = (skey_t *) m->spec[1];
   skey_t *keys_b = (skey_t *) m->spec[2];
-  int imax;
+  int imax, i0 = -1;
   size_t cnt = 0;
   for (imax = 0; imax < EZ_NLOGB; imax++) {
+    if (i0 < 0 && h[imax]) i0 = imax;
     cnt += h[imax];
     if (cnt >= ncell) break;
   }
   const real ilogb_max = 5;
   const real cut = (imax == EZ_NLOGB - 1) ? (real) EZ_REAL_MIN
       : (real) pow(2.0, (double) ilogb_max - imax);
-  cudaMemsetAsync(ps.counter, 0, 8, st);
-  CandBuf none = {nullptr, nullptr, 0, false};
-  CandBuf &c = cb ? *cb : none;
-  compact_kernel<<<(unsigned) ((N + CH - 1) / CH), NT, 0, st>>>(rhot, N, cut, keys_a,
-      ps.counter, c.key, c.idx, c.cap, ps.cstart, ps.ccnt); ez_count_launch();
   // The candidate count is known without waiting for the compaction: a
   // cell's histogram bin is 5 - ilogb(rho_t) (clamped), so for a cut below
   // the last bin, bin <= imax exactly when rho_t >= 2^(5 - imax) = cut, and
   // the candidates are the cells counted in bins 0..imax (cells that are not
   // valid have rho_t = 0 and are in no bin).  The device counter is checked
   // against it at the boundaries' read-back below.  With the cut in the last
-  // bin (zero and subnormal rho_t) the count is read back.
+  // bin (zero and subnormal rho_t) the count is read back and the keys are
+  // sorted.
+  const bool buckets = !m->sel_sort && imax < EZ_NLOGB - 1 && cnt > 0 &&
+      cnt < (1ull << 32) && i0 >= 0;
+  SelBucket sb = {0, 0};
+  if (buckets) {
+    // bucket range: the cut up to the top of bin i0 (2^(6 - i0)); values of
+    // bin 0 above 64 share the last bucket
+    const real upper = (real) pow(2.0, (double) (i0 >= 1 ? 6 - i0 : 6));
+    const ubits_t range = host_bits(upper) - host_bits(cut);
+    sb.base = host_bits(cut);
+    while (((range - 1) >> sb.shift) >= (ubits_t) SEL_NB) sb.shift++;
+    cudaMemsetAsync(ps.bhist, 0, SEL_NB * sizeof(unsigned int), st);
+  }
+  cudaMemsetAsync(ps.counter, 0, 16, st);
+  CandBuf none = {nullptr, nullptr, 0, false};
+  CandBuf &c = cb ? *cb : none;
+  compact_kernel<<<(unsigned) ((N + CH - 1) / CH), NT, 0, st>>>(rhot, N, cut, keys_a,
+      ps.counter, c.key, c.idx, c.cap, ps.cstart, ps.ccnt, buckets ? ps.bhist : nullptr,
+      sb, imax < EZ_NLOGB - 1 ? chist : nullptr, imax); ez_count_launch();
   unsigned long long M = cnt;
   if (imax == EZ_NLOGB - 1 &&
       (!EZ_CUDA_OK(cudaMemcpyAsync(&M, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
        !EZ_CUDA_OK(cudaStreamSynchronize(st))))
     return EZMOCK_ERR_UNKNOWN;
   c.ok = c.key && M <= c.cap;
-  skey_t *sorted = keys_a;
-  if (M > 1) {
-    const size_t ntiles = (M + TILE - 1) / TILE;
-    skey_t *src = keys_a, *dst = keys_b;
-    for (int shift = 0; shift < (int) (8 * sizeof(skey_t)); shift += 8) {
-      digit_hist_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, M, shift, ps.dcount, ntiles); ez_count_launch();
-      scan_u64(ps.dcount, ps.dcscan, 256 * ntiles, ps.tmp, st);
-      digit_scatter_kernel<<<(unsigned) ntiles, SORT_NT, 0, st>>>(src, dst, M, shift, ps.dcscan, ntiles); ez_count_launch();
-      skey_t *t = src; src = dst; dst = t;
-    }
-    sorted = src;
-  }
   // the PDF goes through pinned memory: a pageable upload would wait for
   // the stream (the buffer is reused only after this stage's final wait)
   if (!m->h_small && !EZ_CUDA_OK(cudaMallocHost(&m->h_small, EZ_MAX_NT * sizeof(unsigned long long)))) {
@@ -1286,13 +1561,39 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
   }
   for (int j = 0; j < nmax; j++) m->h_small[j] = pdf[j];
   cudaMemcpyAsync(ps.dpdf, m->h_small, nmax * 8, cudaMemcpyHostToDevice, st);
-  bounds_kernel<<<1, 1, 0, st>>>(sorted, M, ps.dpdf, nmax, ncell, ntot, ps.bo); ez_count_launch();
-  unsigned long long Mdev = 0;
+  if (buckets) {
+    // attributes per call: the kernels may run on several devices
+    cudaFuncSetAttribute(sel_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int) SEL_PLAN_SMEM);
+    cudaFuncSetAttribute(sel_resolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int) SEL_RESOLVE_SMEM);
+    sel_plan_kernel<<<1, SEL_NT, SEL_PLAN_SMEM, st>>>(ps.bhist, M, ps.dpdf, nmax, ps.bmask); ez_count_launch();
+    cudaMemsetAsync(ps.gcount, 0, sizeof(unsigned int), st);
+    const size_t gb = std::min<size_t>((M + NT - 1) / NT, 148 * 8);
+    sel_gather_kernel<<<(unsigned) std::max<size_t>(gb, 1), NT, 0, st>>>(keys_a, M, sb,
+        ps.bmask, ps.gcount, ps.gbuf); ez_count_launch();
+    sel_resolve_kernel<<<1, SEL_NT, SEL_RESOLVE_SMEM, st>>>(ps.bhist, M, sb, ps.gcount,
+        ps.gbuf, ps.dpdf, nmax, ncell, ntot, ps.bo); ez_count_launch();
+  } else {
+    const skey_t *sorted = sort_keys(ps, keys_a, keys_b, M, st);
+    bounds_kernel<<<1, 1, 0, st>>>(sorted, M, ps.dpdf, nmax, ncell, ntot, ps.bo); ez_count_launch();
+  }
+  unsigned long long Mdev[2] = {0, 0};          // candidates, chunks whose count differed
   if (!EZ_CUDA_OK(cudaMemcpyAsync(hb, ps.bo, sizeof(*hb), cudaMemcpyDeviceToHost, st)) ||
-      !EZ_CUDA_OK(cudaMemcpyAsync(&Mdev, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaMemcpyAsync(Mdev, ps.counter, 16, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
     return EZMOCK_ERR_UNKNOWN;
-  if (Mdev != M) return EZMOCK_ERR_UNKNOWN;
+  if (Mdev[0] != M || Mdev[1]) return EZMOCK_ERR_UNKNOWN;
+  m->sel_path = buckets ? 0 : 1;
+  if (buckets && hb->err == SEL_FALLBACK) {
+    m->sel_path = 2;
+    // the marked buckets held more candidates than the gather buffer
+    const skey_t *sorted = sort_keys(ps, keys_a, keys_b, M, st);
+    bounds_kernel<<<1, 1, 0, st>>>(sorted, M, ps.dpdf, nmax, ncell, ntot, ps.bo); ez_count_launch();
+    if (!EZ_CUDA_OK(cudaMemcpyAsync(hb, ps.bo, sizeof(*hb), cudaMemcpyDeviceToHost, st)) ||
+        !EZ_CUDA_OK(cudaStreamSynchronize(st)))
+      return EZMOCK_ERR_UNKNOWN;
+  }
   return 0;
 }
 
@@ -1365,7 +1666,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   if ((e = ez_rng_draws(m, ran, seed, 0, nd_max, m->draws, &dbias))) return e;
   cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
   bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
-      bscan, dbias, ran, (double) (real) EZ_GAUSS_WIDTH, hist); ez_count_launch();
+      bscan, dbias, ran, (double) (real) EZ_GAUSS_WIDTH, hist, ps.chist); ez_count_launch();
   unsigned long long h[EZ_NLOGB], nvalid = 0;
   unsigned int tma_err = 0;        // the field's TMA-staged FFT passes gave up
   if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
@@ -1382,7 +1683,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   ez_stage_begin(m, ST_SELECT);
   HostBounds hb;
   CandBuf cb = cand_buf(m);
-  if ((e = select_stage(m, ps, rhot, h, pdf, nmax, ncell, ntot, &hb, &cb))) return e;
+  if ((e = select_stage(m, ps, rhot, h, pdf, nmax, ncell, ntot, &hb, &cb, ps.chist))) return e;
   ez_stage_end(m, ST_SELECT);
   if (hb.err) { res->err = hb.err; return 0; }
   res->ncell = hb.ncell;

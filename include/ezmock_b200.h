@@ -42,6 +42,12 @@ extern "C" {
    tiles with the Tensor Memory Accelerator on grids of 256^3 and 512^3, 0
    with per-thread asynchronous copies.  Both give the same field. */
 #define EZMOCKB200_OPT_FFT_TMA 8
+/* Boundaries of the PDF bins in the tracer selection: 0 (default) from the
+   candidates' value buckets, sorting only the few buckets that can hold a
+   boundary; 1 from a radix sort of every candidate.  Both give the same
+   counts; the first falls back to the second by itself when the buckets at
+   the boundaries hold too many candidates. */
+#define EZMOCKB200_OPT_SELECT_SORT 9
 
 int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     int *err);
@@ -138,6 +144,12 @@ int EZmockB200_real_size(void);
 
 /* Number of GPU kernels launched by the library in this process. */
 long long EZmockB200_launch_count(void);
+
+/* How the last selection of this instance found the PDF-bin boundaries:
+   0 from the value buckets, 1 from the full sort (requested, or the cut in
+   the last histogram bin), 2 from the full sort after the buckets at the
+   boundaries held too many candidates; -1 before any selection. */
+int EZmockB200_select_path(EZMOCK *ez);
 
 /* Records CUDA event `slot` (0..7) on the instance stream, and the device
    time between two recorded slots (waits for the later one). */

@@ -432,15 +432,22 @@ def test_selection_ties_golden(golden, pk_table):
     assert [nc, no] == list(golden["ties_out"])
 
 
+@pytest.mark.parametrize("sort", [0, 1])
 @pytest.mark.parametrize("prec", [32, 64])
-def test_selection_ties_random(pk_table, prec):
+def test_selection_ties_random(pk_table, prec, sort):
+    """Selection on tracer densities with many ties against the oracle, with
+    the boundaries from the value buckets (option 9 = 0; the heaviest ties
+    overflow the gather buffer and fall back to the full sort) and from the
+    full sort (option 9 = 1)."""
     k, P = pk_table
     Ng = 32
     m = make(prec, Ng, 250.0, 1, 3, k, P)
+    m.set_option(9, sort)
     m.create_dens_field_from_ic()
     O = Oracle(prec)
     rs = np.random.default_rng(5)
     done = 0
+    paths = set()
     for trial in range(10):
         nv = int(rs.choice([300, 3000, 30000]))
         vals = np.exp(rs.uniform(-3, 3.5, nv)).astype(O.rdt)
@@ -459,10 +466,30 @@ def test_selection_ties_random(pk_table, prec):
         assert r == e2
         if r:
             continue
+        paths.add(m.select_path())
         assert np.array_equal(nt, nt_o.reshape(-1))
         assert list(pdf_g) == list(pdf_o) and (nc, no) == (nc_o, no_o)
         done += 1
     assert done >= 3
+    assert paths == ({1} if sort else {0, 2})
+
+
+@pytest.mark.parametrize("Ng,L,n", [(128, 625.0, 2e-4), (256, 1250.0, 2e-4), (128, 625.0, 3e-3)])
+def test_select_buckets_match_sort(pk_table, Ng, L, n):
+    """FP32 catalogues with the selection boundaries from the value buckets
+    (the default, which must not fall back at these densities) and from the
+    full radix sort are identical."""
+    k, P = pk_table
+    m = make(32, Ng, L, 1, 4, k, P)
+    m.create_dens_field_from_ic()
+    nexp = int(n * L ** 3)
+    cats = []
+    for sort in (0, 1):
+        m.set_option(9, sort)
+        cats.append(m.populate_tracer(0.8, 20.0, 0.3, 400.0, nexp))
+        assert m.select_path() == sort
+    for a, b in zip(*cats):
+        assert np.array_equal(a, b)
 
 
 def test_write_ascii(pk_table, tmp_path):
