@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(NT)
 bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
     real thres, double iexp, const unsigned long long *off,
     const uint32_t *__restrict__ draws, int ran, double lambda,
-    unsigned long long *hist, uint16_t *chist) {
+    unsigned long long *hist) {
   constexpr int NW = NT / 32;
   __shared__ unsigned int pre[ROWS * NW];    // valid counts, then prefixes
   __shared__ unsigned int wsum[ROWS * NW / 32];
@@ -247,20 +247,13 @@ bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     if (id < N) rhot[id] = st[q * NT + threadIdx.x];
   }
-  if (threadIdx.x < EZ_NLOGB) {
-    // the chunk's histogram, for the compaction's early reservation
-    chist[(size_t) blockIdx.x * EZ_NLOGB + threadIdx.x] = (uint16_t) sh[threadIdx.x];
-    if (sh[threadIdx.x]) atomicAdd(hist + threadIdx.x, (unsigned long long) sh[threadIdx.x]);
-  }
+  if (threadIdx.x < EZ_NLOGB && sh[threadIdx.x])
+    atomicAdd(hist + threadIdx.x, (unsigned long long) sh[threadIdx.x]);
 }
 
 // Candidates (rho_t >= cut) of a 4096-cell chunk are counted, one atomic per
 // block reserves their slots, and their keys are written (the order of the
-// candidate list is irrelevant: it is sorted next).  With the chunk
-// histograms of the bias stage (chist; cut = 2^(5 - imax) above the last
-// bin, so the candidates are the cells of bins 0..imax) the reservation is
-// made while the chunk's values are still being loaded, and the ballot count
-// is checked against it (counter[1] flags a difference).
+// candidate list is irrelevant: it is sorted next).
 // Value buckets of the candidates for the boundary search below: a monotone
 // map of a candidate's bits (v >= cut > 0, so its bits order as its value),
 // SEL_NB buckets from the cut up; larger values share the last bucket.
@@ -288,15 +281,13 @@ __global__ void __launch_bounds__(NT)
 compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
     skey_t *__restrict__ keys, unsigned long long *counter, skey_t *__restrict__ cand,
     uint16_t *__restrict__ cidx, size_t ccap, unsigned long long *__restrict__ cstart,
-    unsigned int *__restrict__ ccnt, unsigned int *bhist, SelBucket sb,
-    const uint16_t *__restrict__ chist, int imax) {
+    unsigned int *__restrict__ ccnt) {
   // candidates are written warp row by warp row (ballot ranks), so each
   // warp's stores are contiguous; their order within the chunk's range is
   // irrelevant (the keys are sorted, the copies carry their place)
   constexpr int NW = NT / 32;
   __shared__ unsigned int wtot[NW];
-  __shared__ unsigned long long sbase, sres;
-  __shared__ bool sok;
+  __shared__ unsigned long long sbase;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const size_t b0 = (size_t) blockIdx.x * CH;
   real v[ROWS];
@@ -306,16 +297,6 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
   for (int q = 0; q < ROWS; q++) {               // all loads first
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     v[q] = (id < N) ? rhot[id] : (real) 0;
-  }
-  if (chist && w == 0) {                         // reservation while the loads fly
-    const uint16_t *hc = chist + (size_t) blockIdx.x * EZ_NLOGB;
-    unsigned int c = ((lane <= imax) ? hc[lane] : 0u) + ((lane + 32 <= imax) ? hc[lane + 32] : 0u);
-#pragma unroll
-    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) {
-      sres = c;
-      sbase = c ? atomicAdd(counter, (unsigned long long) c) : 0;
-    }
   }
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
@@ -328,18 +309,11 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
   if (threadIdx.x == 0) {
     unsigned long long tot = 0;
     for (int k = 0; k < NW; k++) tot += wtot[k];
-    sok = true;
-    if (!chist) sbase = tot ? atomicAdd(counter, tot) : 0;
-    else if (tot != sres) {
-      atomicAdd(counter + 1, 1ull);            // writes nothing; the stage fails
-      sok = false;
-      tot = 0;
-    }
+    sbase = tot ? atomicAdd(counter, tot) : 0;
     cstart[blockIdx.x] = sbase;
     ccnt[blockIdx.x] = (unsigned int) tot;
   }
   __syncthreads();
-  if (!sok) return;
   unsigned long long off = sbase;
   for (int k = 0; k < w; k++) off += wtot[k];
   const unsigned int lt = (1u << lane) - 1;
@@ -351,7 +325,6 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
       keys[pos] = k;
       // a second copy with the cell's place in the chunk, kept for emission
       if (pos < ccap) { cand[pos] = k; cidx[pos] = (uint16_t) (q * NT + threadIdx.x); }
-      if (bhist) atomicAdd(bhist + sel_bucket(v[q], sb), 1u);
     }
     off += __popc(bal[q]);
   }
@@ -543,47 +516,103 @@ __global__ void bounds_kernel(const skey_t *__restrict__ keys, size_t M,
 // bounds_kernel's on the fully sorted keys; when the marked buckets hold more
 // than SEL_GCAP candidates, sel_resolve_kernel asks for the full sort.
 constexpr int SEL_NT = 1024;
+constexpr int SEL_HB = 148;                               // bucket histogram blocks at most
 constexpr int SEL_GCAP = 65536 / (int) sizeof(skey_t);   // gathered keys (64 KB)
 constexpr int SEL_FALLBACK = -2;                          // BoundOut.err: sort all
 constexpr size_t SEL_PLAN_SMEM = SEL_NB * sizeof(unsigned int);
 constexpr size_t SEL_RESOLVE_SMEM = SEL_PLAN_SMEM + SEL_GCAP * sizeof(skey_t);
 
 // cum[b] = candidates in buckets above b (exclusive prefix in descending
-// bucket order); returns the total.  All threads; ends with a barrier.
+// bucket order); returns the total.  Warp w scans the 1024 buckets of places
+// w*1024 .. w*1024+1023 in descending order (coalesced reads), then adds the
+// counts of the warps before it.  All threads; ends with a barrier.
 __device__ unsigned int sel_cum(const unsigned int *__restrict__ bh, unsigned int *cum,
     unsigned int *sw) {
-  constexpr int PER = SEL_NB / SEL_NT;
-  unsigned int c[PER], s = 0;
+  constexpr int SEG = SEL_NB / (SEL_NT / 32);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned int run = 0;
+#pragma unroll 8
+  for (int i = 0; i < SEG / 32; i++) {
+    const int b = SEL_NB - 1 - (w * SEG + i * 32 + lane);
+    const unsigned int c = bh[b];
+    unsigned int x = c;
 #pragma unroll
-  for (int i = 0; i < PER; i++) {
-    c[i] = bh[SEL_NB - 1 - (threadIdx.x * PER + i)];
-    s += c[i];
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    cum[b] = run + x - c;
+    run += __shfl_sync(0xffffffffu, x, 31);
   }
-  unsigned int tot;
-  unsigned int run = block_scan<unsigned int>(s, &tot, sw);
-#pragma unroll
-  for (int i = 0; i < PER; i++) {
-    cum[SEL_NB - 1 - (threadIdx.x * PER + i)] = run;
-    run += c[i];
+  if (lane == 0) sw[w] = run;
+  __syncthreads();
+  unsigned int off = 0, tot = 0;
+  for (int k = 0; k < SEL_NT / 32; k++) {
+    const unsigned int v = sw[k];
+    off += (k < w) ? v : 0u;
+    tot += v;
   }
+  if (off)
+    for (int i = 0; i < SEG / 32; i++) cum[SEL_NB - 1 - (w * SEG + i * 32 + lane)] += off;
   __syncthreads();
   return tot;
 }
 
-// Bucket of rank r: the lowest b with cum[b] <= r (cum does not increase
-// with b; that b is non-empty).
-__device__ __forceinline__ int sel_rank_bucket(const unsigned int *cum, unsigned long long r) {
-  int lo = 0, hi = SEL_NB - 1;
+// First i in [0, n) with pred(i) (pred false then true), n if none: a
+// 32-way search by one warp; every lane returns the answer.
+template <class Pred>
+__device__ __forceinline__ int warp_first(int n, Pred pred, int lane) {
+  int lo = 0, hi = n;            // pred false below lo; true at hi (or hi = n)
   while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (cum[mid] <= r) hi = mid; else lo = mid + 1;
+    const int step = (hi - lo + 31) >> 5;
+    const int idx = lo + (lane + 1) * step - 1;
+    const unsigned int bal = __ballot_sync(0xffffffffu, idx >= hi || pred(idx));
+    if (!bal) { lo = hi; break; }
+    const int f = __ffs(bal) - 1;
+    const int nhi = lo + (f + 1) * step - 1;
+    lo += f * step;
+    hi = nhi < hi ? nhi : hi;
   }
   return lo;
+}
+
+// Bucket of rank r: the lowest b with cum[b] <= r (cum does not increase
+// with b; that b is non-empty).
+__device__ __forceinline__ int sel_rank_bucket(const unsigned int *cum, unsigned long long r,
+    int lane) {
+  return warp_first(SEL_NB, [&](int b) { return cum[b] <= r; }, lane);
 }
 
 __device__ __forceinline__ unsigned long long sel_bucket_end(const unsigned int *cum, int b,
     unsigned long long M) {
   return b > 0 ? cum[b - 1] : M;
+}
+
+// Per-block histograms of the candidates' buckets (shared-memory atomics),
+// then their sum: SEL_NB counts.
+__global__ void __launch_bounds__(SEL_NT)
+sel_hist_kernel(const skey_t *__restrict__ keys, size_t M, SelBucket sb, unsigned int *part) {
+  extern __shared__ unsigned int hb[];              // SEL_NB
+  for (int e = threadIdx.x; e < SEL_NB; e += SEL_NT) hb[e] = 0;
+  __syncthreads();
+  const size_t per = (M + gridDim.x - 1) / gridDim.x;
+  const size_t a = (size_t) blockIdx.x * per, b = min(M, a + per);
+#pragma unroll 4
+  for (size_t i = a + threadIdx.x; i < b; i += SEL_NT)
+    atomicAdd(&hb[sel_bucket(from_key(keys[i]), sb)], 1u);
+  __syncthreads();
+  unsigned int *o = part + (size_t) blockIdx.x * SEL_NB;
+  for (int e = threadIdx.x; e < SEL_NB; e += SEL_NT) o[e] = hb[e];
+}
+
+__global__ void __launch_bounds__(NT)
+sel_reduce_kernel(const unsigned int *__restrict__ part, int nparts, unsigned int *bh) {
+  const int e = blockIdx.x * NT + threadIdx.x;
+  if (e >= SEL_NB) return;
+  unsigned int s = 0;
+#pragma unroll 8
+  for (int p = 0; p < nparts; p++) s += part[(size_t) p * SEL_NB + e];
+  bh[e] = s;
 }
 
 __global__ void __launch_bounds__(SEL_NT)
@@ -592,22 +621,26 @@ sel_plan_kernel(const unsigned int *__restrict__ bh, unsigned long long M,
   extern __shared__ unsigned int cum[];             // SEL_NB
   __shared__ unsigned int sw[32];
   __shared__ unsigned int mask[SEL_NB / 32];
+  __shared__ unsigned long long spdf[EZ_MAX_NT];
   for (int w = threadIdx.x; w < SEL_NB / 32; w += SEL_NT) mask[w] = 0;
+  for (int j = threadIdx.x; j < nmax; j += SEL_NT) spdf[j] = pdf[j];
   sel_cum(bh, cum, sw);
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {                           // one warp follows the chain
+    const int lane = threadIdx.x;
     unsigned long long plo = 0, phi = 0;
     for (int j = 0; j < nmax; j++) {
-      const unsigned long long q = pdf[j];
+      const unsigned long long q = spdf[j];
       if (!q) continue;
       const unsigned long long elo = plo + q;
       if (elo > M) break;                            // the exact chain fails here
       const unsigned long long ehi = min(phi + q, M);
-      const int bhi = sel_rank_bucket(cum, elo - 1);  // higher values, higher bucket
-      const int blo = sel_rank_bucket(cum, ehi - 1);
-      for (int w = blo >> 5; w <= (bhi >> 5); w++) {
+      const int bhi = sel_rank_bucket(cum, elo - 1, lane);   // higher values, higher bucket
+      const int blo = sel_rank_bucket(cum, ehi - 1, lane);
+      for (int w = (blo >> 5) + lane; w <= (bhi >> 5); w += 32) {
         const int a = max(blo - 32 * w, 0), b = min(bhi - 32 * w, 31);
         mask[w] |= (b == 31 ? 0xffffffffu : ((2u << b) - 1)) & ~((1u << a) - 1);
       }
+      __syncwarp();
       plo = elo;
       phi = sel_bucket_end(cum, blo, M);
     }
@@ -652,6 +685,8 @@ sel_resolve_kernel(const unsigned int *__restrict__ bh, unsigned long long M, Se
   extern __shared__ unsigned int cum[];             // SEL_NB, then the keys
   skey_t *g = reinterpret_cast<skey_t *>(cum + SEL_NB);
   __shared__ unsigned int sw[32];
+  __shared__ unsigned long long spdf[EZ_MAX_NT];
+  for (int j = threadIdx.x; j < nmax; j += SEL_NT) spdf[j] = pdf[j];
   const unsigned int tot = sel_cum(bh, cum, sw);
   const unsigned int G = *gcount;
   if (tot != M || G > (unsigned int) SEL_GCAP) {     // uniform over the block
@@ -674,43 +709,54 @@ sel_resolve_kernel(const unsigned int *__restrict__ bh, unsigned long long M, Se
       }
       __syncthreads();
     }
-  if (threadIdx.x) return;
-  // bounds_kernel's chain; the key of rank r is found in the sorted gathered
-  // keys: its bucket b's keys start at the first key with bucket <= b
+  if (threadIdx.x >= 32) return;
+  // bounds_kernel's chain, one warp; the key of rank r is found in the sorted
+  // gathered keys: its bucket b's keys start at the first key with bucket <= b
+  const int lane = threadIdx.x;
   unsigned long long P = 0;
   int nb = 0;
   for (int j = 0; j < nmax; j++) {
-    unsigned long long q = pdf[j];
-    if (!q) { o->pdf[j] = 0; continue; }
+    unsigned long long q = spdf[j];
+    if (!q) { if (!lane) o->pdf[j] = 0; continue; }
     unsigned long long E = P + q;
-    if (E > M) { o->err = EZMOCK_ERR_UNKNOWN; return; }
-    const int b = sel_rank_bucket(cum, E - 1);
-    int lo = 0, hi = (int) G;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (sel_bucket(from_key(g[mid]), sb) <= b) hi = mid; else lo = mid + 1;
-    }
+    if (E > M) { if (!lane) o->err = EZMOCK_ERR_UNKNOWN; return; }
+    const int b = sel_rank_bucket(cum, E - 1, lane);
+    const int lo = warp_first((int) G, [&](int i) { return sel_bucket(from_key(g[i]), sb) <= b; },
+        lane);
     const unsigned long long i = lo + (E - 1 - cum[b]);
-    if (i >= G || sel_bucket(from_key(g[i]), sb) != b) { o->err = SEL_FALLBACK; return; }
+    if (i >= G || sel_bucket(from_key(g[i]), sb) != b) {
+      if (!lane) o->err = SEL_FALLBACK;
+      return;
+    }
     const skey_t kv = g[i];
-    unsigned long long ie = i;
-    while (ie + 1 < G && g[ie + 1] == kv) ie++;
+    unsigned long long ie = i;                     // last key equal to kv
+    for (;;) {
+      const unsigned long long t = ie + 1 + lane;
+      const unsigned int eq = __ballot_sync(0xffffffffu, t < G && g[t] == kv);
+      if (eq == 0xffffffffu) { ie += 32; continue; }
+      ie += __ffs(~eq) - 1;
+      break;
+    }
     const unsigned long long E2 = cum[b] + (ie - lo) + 1;
     const unsigned long long extra = E2 - E;
     q += extra;
     ncell += extra;
     ntot += extra * (unsigned long long) (nmax - j);
     E = E2;
-    o->pdf[j] = q;
-    o->lo[nb] = from_key(kv);
-    o->ntr[nb] = nmax - j;
+    if (!lane) {
+      o->pdf[j] = q;
+      o->lo[nb] = from_key(kv);
+      o->ntr[nb] = nmax - j;
+    }
     nb++;
     P = E;
   }
-  o->nbins = nb;
-  o->ncell = ncell;
-  o->ntot = ntot;
-  o->err = 0;
+  if (!lane) {
+    o->nbins = nb;
+    o->ncell = ncell;
+    o->ntot = ntot;
+    o->err = 0;
+  }
 }
 
 __device__ __forceinline__ int cell_count(real v, const real *lo, const int *ntr,
@@ -1408,7 +1454,7 @@ struct PopScratch {
   unsigned int *bmask;          // SEL_NB bits: buckets that can hold a boundary
   unsigned int *gcount;         // candidates of the marked buckets
   skey_t *gbuf;                 // their keys (SEL_GCAP)
-  uint16_t *chist;              // per chunk: log2 histogram of rho_t (bias stage)
+  unsigned int *bpart;          // per-block bucket histograms (SEL_HB x SEL_NB)
 };
 
 // Candidate copies for emission, in the draws buffer (free between the bias
@@ -1449,8 +1495,8 @@ int pop_scratch(EzMesh *m, PopScratch *ps) {
   const size_t off_bm = off_bh + SEL_NB * 4;
   const size_t off_gc = off_bm + SEL_NB / 8;
   const size_t off_gb = off_gc + 256;
-  const size_t off_ch = (off_gb + SEL_GCAP * sizeof(skey_t) + 255) / 256 * 256;
-  int e = ez_scratch(m, off_ch + nblk * EZ_NLOGB * sizeof(uint16_t));
+  const size_t off_bp = (off_gb + SEL_GCAP * sizeof(skey_t) + 255) / 256 * 256;
+  int e = ez_scratch(m, off_bp + (size_t) SEL_HB * SEL_NB * sizeof(unsigned int));
   if (e) return e;
   char *sc = (char *) m->scratch;
   ps->bcnt = (unsigned long long *) (sc + off_cnt);
@@ -1468,7 +1514,7 @@ int pop_scratch(EzMesh *m, PopScratch *ps) {
   ps->bmask = (unsigned int *) (sc + off_bm);
   ps->gcount = (unsigned int *) (sc + off_gc);
   ps->gbuf = (skey_t *) (sc + off_gb);
-  ps->chist = (uint16_t *) (sc + off_ch);
+  ps->bpart = (unsigned int *) (sc + off_bp);
   return 0;
 }
 
@@ -1506,7 +1552,7 @@ ubits_t host_bits(real v) {
 // the device.
 int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
     const unsigned long long *h, const size_t *pdf, int nmax, size_t ncell,
-    size_t ntot, HostBounds *hb, CandBuf *cb = nullptr, const uint16_t *chist = nullptr) {
+    size_t ntot, HostBounds *hb, CandBuf *cb = nullptr) {
   const size_t N = m->N;
   cudaStream_t st = m->stream;
   skey_t *keys_a = (skey_t *) m->spec[1];
@@ -1539,14 +1585,12 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
     const ubits_t range = host_bits(upper) - host_bits(cut);
     sb.base = host_bits(cut);
     while (((range - 1) >> sb.shift) >= (ubits_t) SEL_NB) sb.shift++;
-    cudaMemsetAsync(ps.bhist, 0, SEL_NB * sizeof(unsigned int), st);
   }
-  cudaMemsetAsync(ps.counter, 0, 16, st);
+  cudaMemsetAsync(ps.counter, 0, 8, st);
   CandBuf none = {nullptr, nullptr, 0, false};
   CandBuf &c = cb ? *cb : none;
   compact_kernel<<<(unsigned) ((N + CH - 1) / CH), NT, 0, st>>>(rhot, N, cut, keys_a,
-      ps.counter, c.key, c.idx, c.cap, ps.cstart, ps.ccnt, buckets ? ps.bhist : nullptr,
-      sb, imax < EZ_NLOGB - 1 ? chist : nullptr, imax); ez_count_launch();
+      ps.counter, c.key, c.idx, c.cap, ps.cstart, ps.ccnt); ez_count_launch();
   unsigned long long M = cnt;
   if (imax == EZ_NLOGB - 1 &&
       (!EZ_CUDA_OK(cudaMemcpyAsync(&M, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
@@ -1563,10 +1607,15 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
   cudaMemcpyAsync(ps.dpdf, m->h_small, nmax * 8, cudaMemcpyHostToDevice, st);
   if (buckets) {
     // attributes per call: the kernels may run on several devices
+    cudaFuncSetAttribute(sel_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int) SEL_PLAN_SMEM);
     cudaFuncSetAttribute(sel_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int) SEL_PLAN_SMEM);
     cudaFuncSetAttribute(sel_resolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int) SEL_RESOLVE_SMEM);
+    const int nh = (int) std::min<size_t>((M + 8191) / 8192, SEL_HB);
+    sel_hist_kernel<<<nh, SEL_NT, SEL_PLAN_SMEM, st>>>(keys_a, M, sb, ps.bpart); ez_count_launch();
+    sel_reduce_kernel<<<SEL_NB / NT, NT, 0, st>>>(ps.bpart, nh, ps.bhist); ez_count_launch();
     sel_plan_kernel<<<1, SEL_NT, SEL_PLAN_SMEM, st>>>(ps.bhist, M, ps.dpdf, nmax, ps.bmask); ez_count_launch();
     cudaMemsetAsync(ps.gcount, 0, sizeof(unsigned int), st);
     const size_t gb = std::min<size_t>((M + NT - 1) / NT, 148 * 8);
@@ -1578,12 +1627,12 @@ int select_stage(EzMesh *m, const PopScratch &ps, const real *rhot,
     const skey_t *sorted = sort_keys(ps, keys_a, keys_b, M, st);
     bounds_kernel<<<1, 1, 0, st>>>(sorted, M, ps.dpdf, nmax, ncell, ntot, ps.bo); ez_count_launch();
   }
-  unsigned long long Mdev[2] = {0, 0};          // candidates, chunks whose count differed
+  unsigned long long Mdev = 0;
   if (!EZ_CUDA_OK(cudaMemcpyAsync(hb, ps.bo, sizeof(*hb), cudaMemcpyDeviceToHost, st)) ||
-      !EZ_CUDA_OK(cudaMemcpyAsync(Mdev, ps.counter, 16, cudaMemcpyDeviceToHost, st)) ||
+      !EZ_CUDA_OK(cudaMemcpyAsync(&Mdev, ps.counter, 8, cudaMemcpyDeviceToHost, st)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(st)))
     return EZMOCK_ERR_UNKNOWN;
-  if (Mdev[0] != M || Mdev[1]) return EZMOCK_ERR_UNKNOWN;
+  if (Mdev != M) return EZMOCK_ERR_UNKNOWN;
   m->sel_path = buckets ? 0 : 1;
   if (buckets && hb->err == SEL_FALLBACK) {
     m->sel_path = 2;
@@ -1666,7 +1715,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   if ((e = ez_rng_draws(m, ran, seed, 0, nd_max, m->draws, &dbias))) return e;
   cudaMemsetAsync(hist, 0, EZ_NLOGB * 8, st);
   bias_kernel<<<(unsigned) nblk, NT, 0, st>>>(m->rho, rhot, N, thres, iexp,
-      bscan, dbias, ran, (double) (real) EZ_GAUSS_WIDTH, hist, ps.chist); ez_count_launch();
+      bscan, dbias, ran, (double) (real) EZ_GAUSS_WIDTH, hist); ez_count_launch();
   unsigned long long h[EZ_NLOGB], nvalid = 0;
   unsigned int tma_err = 0;        // the field's TMA-staged FFT passes gave up
   if (!EZ_CUDA_OK(cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, st)) ||
@@ -1683,7 +1732,7 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   ez_stage_begin(m, ST_SELECT);
   HostBounds hb;
   CandBuf cb = cand_buf(m);
-  if ((e = select_stage(m, ps, rhot, h, pdf, nmax, ncell, ntot, &hb, &cb, ps.chist))) return e;
+  if ((e = select_stage(m, ps, rhot, h, pdf, nmax, ncell, ntot, &hb, &cb))) return e;
   ez_stage_end(m, ST_SELECT);
   if (hb.err) { res->err = hb.err; return 0; }
   res->ncell = hb.ncell;

@@ -471,7 +471,43 @@ def test_selection_ties_random(pk_table, prec, sort):
         assert list(pdf_g) == list(pdf_o) and (nc, no) == (nc_o, no_o)
         done += 1
     assert done >= 3
-    assert paths == ({1} if sort else {0, 2})
+    if sort:
+        assert paths == {1}
+    else:
+        assert 0 in paths and paths <= {0, 2}
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+def test_selection_tie_flood(pk_table, prec):
+    """A PDF-bin boundary inside a run of 17000 equal tracer densities: the
+    bucket search finds more candidates in the boundary's bucket than it
+    gathers, falls back to the full sort (path 2), and the counts equal the
+    oracle's and the full sort's."""
+    k, P = pk_table
+    Ng = 32
+    m = make(prec, Ng, 250.0, 1, 3, k, P)
+    m.create_dens_field_from_ic()
+    O = Oracle(prec)
+    rs = np.random.default_rng(11)
+    rhot = np.zeros(Ng ** 3, O.rdt)
+    cells = rs.permutation(Ng ** 3)
+    rhot[cells[:200]] = rs.uniform(2.0, 8.0, 200)
+    rhot[cells[200:17200]] = 1.5
+    rhot[cells[17200:27200]] = rs.uniform(1.0, 1.5, 10000)
+    lb = np.floor(np.log2(rhot[rhot > 0].astype(np.float64))).astype(int)
+    hist = np.zeros(64, np.uintp)
+    np.add.at(hist, np.clip(5 - lb, 0, 63), 1)
+    pdf = [50, 400, 3000]
+    ncell, ntot = sum(pdf), 50 * 3 + 400 * 2 + 3000
+    e2, nt_o, pdf_o, nc_o, no_o = O.select(Ng, rhot.reshape(Ng, Ng, Ng), hist, pdf, 3,
+                                           ncell, ntot)
+    assert e2 == 0 and nc_o == 200 + 17000 + 3000
+    for sort, path in ((0, 2), (1, 1)):
+        m.set_option(9, sort)
+        r, nt, pdf_g, nc, no = _select(m, prec, rhot, hist, pdf, 3, ncell, ntot)
+        assert r == 0 and m.select_path() == path
+        assert np.array_equal(nt, nt_o.reshape(-1))
+        assert list(pdf_g) == list(pdf_o) and (nc, no) == (nc_o, no_o)
 
 
 @pytest.mark.parametrize("Ng,L,n", [(128, 625.0, 2e-4), (256, 1250.0, 2e-4), (128, 625.0, 3e-3)])
