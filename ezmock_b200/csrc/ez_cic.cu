@@ -322,22 +322,6 @@ constexpr int TSLOT = TX * TY;                // ints per slice and quantity
 constexpr int TQS = TRS * TSLOT;              // ints per quantity
 constexpr int TNT = 480;                      // threads: two columns each
 constexpr size_t TSMEM = 4 * (size_t) TQS * sizeof(int);
-// Packed rings: (rho, q0) and (q1, q2) as the two halves of 64-bit words,
-// one red.shared.add.u64 per pair.  The low half is sign-extended into the
-// high one, so the 64-bit sum is hi_sum * 2^32 + lo_sum exactly; with
-// lo_sum in the int32 range (the same bound as the 32-bit rings) the low
-// half of the sum is lo_sum and hi_sum = (sum - lo_sum) / 2^32.  PK = 2
-// alternates the pair a lane deposits first with the lane's parity and puts
-// the second pair plane 16 banks further, so that lanes of a half-warp that
-// land on one cell hit different banks.
-constexpr size_t TPQ = (size_t) TQS * sizeof(unsigned long long);   // bytes per pair plane
-template <int PK>
-__host__ __device__ constexpr size_t tile_pair_off() { return PK == 2 ? TPQ + 64 : TPQ; }
-template <int PK>
-__host__ __device__ constexpr size_t tile_smem() { return PK ? tile_pair_off<PK>() + TPQ : TSMEM; }
-#ifndef EZ_CIC_PACK
-#define EZ_CIC_PACK 0
-#endif
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t) __cvta_generic_to_shared(p);
@@ -347,21 +331,7 @@ __device__ __forceinline__ void red_add(uint32_t addr, int v) {
   asm volatile("red.shared.add.s32 [%0], %1;" :: "r"(addr), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ void red_add64(uint32_t addr, unsigned long long v) {
-  asm volatile("red.shared.add.u64 [%0], %1;" :: "r"(addr), "l"(v) : "memory");
-}
-
-// (hi, lo) as hi * 2^32 + lo in 64-bit two's complement
-__device__ __forceinline__ unsigned long long pack2(int lo, int hi) {
-  return ((unsigned long long) (unsigned int) hi << 32) + (unsigned long long) (long long) lo;
-}
-
-__device__ __forceinline__ void unpack2(unsigned long long v, int &lo, int &hi) {
-  lo = (int) (unsigned int) v;
-  hi = (int) ((long long) (v - (unsigned long long) (long long) lo) >> 32);
-}
-
-template <int OH, int PK>
+template <int OH>
 __global__ void __launch_bounds__(TNT, 1)
 cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
     const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
@@ -384,7 +354,7 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
   const float pmax = fmaxf(__uint_as_float(stats->psimax_bits), 1e-30f);
   const float mscale = exp2f(floorf(log2f(2147483647.f / (1024.f * pmax))));
   const float minv = 1.f / mscale;
-  for (int e = threadIdx.x; e < (int) (tile_smem<PK>() / 16); e += TNT)
+  for (int e = threadIdx.x; e < TQS; e += TNT)      // 4 * TQS ints as int4
     reinterpret_cast<int4 *>(tring)[e] = make_int4(0, 0, 0, 0);
 
   // the thread's two columns (the second may be past the last one)
@@ -482,36 +452,24 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
         r0 -= (r0 >= TRS) ? TRS : 0;
         int r1 = r0 + 1;
         r1 -= (r1 >= TRS) ? TRS : 0;
-        constexpr uint32_t ES = PK ? 8u : 4u;     // bytes per ring entry
-        const uint32_t cell = ringb + ES * (uint32_t) (cx * TY + cy);
-        const uint32_t b0 = cell + ES * (uint32_t) (r0 * TSLOT);
-        const uint32_t b1 = cell + ES * (uint32_t) (r1 * TSLOT);
+        const uint32_t cell = ringb + 4u * (uint32_t) (cx * TY + cy);
+        const uint32_t b0 = cell + 4u * (uint32_t) (r0 * TSLOT);
+        const uint32_t b1 = cell + 4u * (uint32_t) (r1 * TSLOT);
         const float sm1 = pa * mscale, sm2 = pb * mscale, sm3 = pc * mscale;
         const float zq[2][4] = {{wz0 * RHO_SCALE, wz0 * sm1, wz0 * sm2, wz0 * sm3},
                                 {wz1 * RHO_SCALE, wz1 * sm1, wz1 * sm2, wz1 * sm3}};
         const float wxy[4] = {wx0 * wy0, wx0 * wy1, wx1 * wy0, wx1 * wy1};
         const bool ok[4] = {ax0 && by0, ax0 && by1, ax1 && by0, ax1 && by1};
         constexpr uint32_t QB = 4u * TQS;
-        constexpr uint32_t PB = (uint32_t) tile_pair_off<PK>();
-        const bool odd = PK == 2 && (threadIdx.x & 1);
 #pragma unroll
         for (int ab = 0; ab < 4; ab++) {
           if (!ok[ab]) continue;
-          const uint32_t off = ES * (uint32_t) ((ab >> 1) * TY + (ab & 1));
+          const uint32_t off = 4u * (uint32_t) ((ab >> 1) * TY + (ab & 1));
 #pragma unroll
           for (int ic = 0; ic < 2; ic++) {
             const uint32_t r = (ic ? b1 : b0) + off;
-            if (PK == 0) {
 #pragma unroll
-              for (int q = 0; q < 4; q++) red_add(r + q * QB, fmround(wxy[ab], zq[ic][q]));
-            } else {
-              const unsigned long long v0 = pack2(fmround(wxy[ab], zq[ic][0]),
-                                                  fmround(wxy[ab], zq[ic][1]));
-              const unsigned long long v1 = pack2(fmround(wxy[ab], zq[ic][2]),
-                                                  fmround(wxy[ab], zq[ic][3]));
-              red_add64(odd ? r + PB : r, odd ? v1 : v0);
-              red_add64(odd ? r : r + PB, odd ? v0 : v1);
-            }
+            for (int q = 0; q < 4; q++) red_add(r + q * QB, fmround(wxy[ab], zq[ic][q]));
           }
         }
       }
@@ -521,44 +479,19 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
     __syncthreads();
     const int zo = (p - 1) * TZ;
     const bool wr = zo >= zs && zo < ze;
-    if (PK == 0) {
-      for (int t = threadIdx.x; t < 4 * TSLOT; t += TNT) {
-        const int q = t / TSLOT, cc = t - q * TSLOT;
-        int *src = tring + q * TQS + rbase * TSLOT + cc;
-        int v[TZ];
+    for (int t = threadIdx.x; t < 4 * TSLOT; t += TNT) {
+      const int q = t / TSLOT, cc = t - q * TSLOT;
+      int *src = tring + q * TQS + rbase * TSLOT + cc;
+      int v[TZ];
 #pragma unroll
-        for (int kk = 0; kk < TZ; kk++) { v[kk] = src[kk * TSLOT]; src[kk * TSLOT] = 0; }
-        if (wr) {
-          const float f = (q == 0) ? (1.f / RHO_SCALE) : minv;
-          real *g = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
-          const int cx = cc / TY, cy = cc - (cc / TY) * TY;
-          float4 *dst = reinterpret_cast<float4 *>(g + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo);
-          dst[0] = make_float4(v[0] * f, v[1] * f, v[2] * f, v[3] * f);
-          dst[1] = make_float4(v[4] * f, v[5] * f, v[6] * f, v[7] * f);
-        }
-      }
-    } else {
-      for (int t = threadIdx.x; t < 2 * TSLOT; t += TNT) {
-        const int pr = t / TSLOT, cc = t - pr * TSLOT;
-        unsigned long long *src = reinterpret_cast<unsigned long long *>(
-            reinterpret_cast<char *>(tring) + pr * tile_pair_off<PK>()) + rbase * TSLOT + cc;
-        int lo[TZ], hi[TZ];
-#pragma unroll
-        for (int kk = 0; kk < TZ; kk++) {
-          unpack2(src[kk * TSLOT], lo[kk], hi[kk]);
-          src[kk * TSLOT] = 0ull;
-        }
-        if (wr) {
-          const float fl = pr ? minv : (1.f / RHO_SCALE);
-          real *gl = pr ? q1 : rho, *gh = pr ? q2 : q0;
-          const int cx = cc / TY, cy = cc - (cc / TY) * TY;
-          const size_t o = ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo;
-          float4 *dl = reinterpret_cast<float4 *>(gl + o), *dh = reinterpret_cast<float4 *>(gh + o);
-          dl[0] = make_float4(lo[0] * fl, lo[1] * fl, lo[2] * fl, lo[3] * fl);
-          dl[1] = make_float4(lo[4] * fl, lo[5] * fl, lo[6] * fl, lo[7] * fl);
-          dh[0] = make_float4(hi[0] * minv, hi[1] * minv, hi[2] * minv, hi[3] * minv);
-          dh[1] = make_float4(hi[4] * minv, hi[5] * minv, hi[6] * minv, hi[7] * minv);
-        }
+      for (int kk = 0; kk < TZ; kk++) { v[kk] = src[kk * TSLOT]; src[kk * TSLOT] = 0; }
+      if (wr) {
+        const float f = (q == 0) ? (1.f / RHO_SCALE) : minv;
+        real *g = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
+        const int cx = cc / TY, cy = cc - (cc / TY) * TY;
+        float4 *dst = reinterpret_cast<float4 *>(g + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo);
+        dst[0] = make_float4(v[0] * f, v[1] * f, v[2] * f, v[3] * f);
+        dst[1] = make_float4(v[4] * f, v[5] * f, v[6] * f, v[7] * f);
       }
     }
     __syncthreads();
@@ -708,12 +641,10 @@ int ez_cic(EzMesh *m, double Lbox) {
         // 16 x 32 tiles; the z range is cut so that the CTAs (one per SM)
         // fill whole waves: pick the cut count with the least time per
         // wave-slot, counting each range's two extra steps
-        constexpr int PK = EZ_CIC_PACK;
-        constexpr size_t TSM = tile_smem<PK>();
-        if (!EZ_CUDA_OK(cudaFuncSetAttribute(cic_tile_kernel<2, PK>,
-                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) TSM)) ||
-            !EZ_CUDA_OK(cudaFuncSetAttribute(cic_tile_kernel<3, PK>,
-                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) TSM)))
+        if (!EZ_CUDA_OK(cudaFuncSetAttribute(cic_tile_kernel<2>,
+                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) TSMEM)) ||
+            !EZ_CUDA_OK(cudaFuncSetAttribute(cic_tile_kernel<3>,
+                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) TSMEM)))
           return EZMOCK_ERR_UNKNOWN;
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
@@ -728,10 +659,10 @@ int ez_cic(EzMesh *m, double Lbox) {
         }
         const unsigned nblk = (unsigned) (tiles * nzs);
         if (m->cic_oh != 2)
-          cic_tile_kernel<3, PK><<<nblk, TNT, TSM, m->stream>>>(m->psi[0], m->psi[1],
+          cic_tile_kernel<3><<<nblk, TNT, TSMEM, m->stream>>>(m->psi[0], m->psi[1],
               m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list, nzs);
         else
-          cic_tile_kernel<2, PK><<<nblk, TNT, TSM, m->stream>>>(m->psi[0], m->psi[1],
+          cic_tile_kernel<2><<<nblk, TNT, TSMEM, m->stream>>>(m->psi[0], m->psi[1],
               m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list, nzs);
       }
       else {
