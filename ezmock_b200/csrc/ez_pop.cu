@@ -84,32 +84,49 @@ valid_count_kernel(const real *__restrict__ rho, size_t N, real thres,
   if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
 }
 
-// single-block exclusive scan of n values; out[n] = total.  Each thread's
-// segment is read in batches of eight independent loads (a loop of single
-// loads was a chain of L2 latencies).
+// single-block exclusive scan of n values (in place allowed); out[n] =
+// total.  Warp w owns the w-th of 32 contiguous segments: it sums its
+// segment with coalesced loads (eight in flight per lane), the warp totals
+// are scanned, and each warp rescans its segment 32 values at a time.
 __global__ void __launch_bounds__(1024)
-scan_kernel(const unsigned long long *__restrict__ in, unsigned long long *out,
-    size_t n) {
+scan_kernel(const unsigned long long *in, unsigned long long *out, size_t n) {
   __shared__ unsigned long long sw[32];
-  const size_t per = (n + blockDim.x - 1) / blockDim.x;
-  const size_t s0 = threadIdx.x * per, s1 = min(n, s0 + per);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const size_t seg = ((n + 31) / 32 + 31) & ~(size_t) 31;
+  const size_t s0 = min(n, (size_t) w * seg), s1 = min(n, s0 + seg);
   unsigned long long loc = 0;
-  for (size_t b = s0; b < s1; b += 8) {
+  for (size_t b = s0; b < s1; b += 8 * 32) {
     unsigned long long v[8];
 #pragma unroll
-    for (int u = 0; u < 8; u++) v[u] = (b + u < s1) ? in[b + u] : 0ull;
+    for (int u = 0; u < 8; u++) {
+      const size_t g = b + (size_t) u * 32 + lane;
+      v[u] = (g < s1) ? in[g] : 0ull;
+    }
 #pragma unroll
     for (int u = 0; u < 8; u++) loc += v[u];
   }
-  unsigned long long tot;
-  unsigned long long run = block_scan<unsigned long long>(loc, &tot, sw);
-  for (size_t b = s0; b < s1; b += 8) {
-    unsigned long long v[8];
 #pragma unroll
-    for (int u = 0; u < 8; u++) v[u] = (b + u < s1) ? in[b + u] : 0ull;
+  for (int o = 16; o; o >>= 1) loc += __shfl_xor_sync(0xffffffffu, loc, o);
+  if (lane == 0) sw[w] = loc;
+  __syncthreads();
+  unsigned long long run = 0, tot = 0;
+  for (int k = 0; k < 32; k++) {
+    const unsigned long long t = sw[k];
+    run += (k < w) ? t : 0ull;
+    tot += t;
+  }
+  __syncthreads();                               // all reads of `in` done before
+  for (size_t b = s0; b < s1; b += 32) {         // in-place writes
+    const size_t g = b + lane;
+    const unsigned long long v = (g < s1) ? in[g] : 0ull;
+    unsigned long long x = v;
 #pragma unroll
-    for (int u = 0; u < 8; u++)
-      if (b + u < s1) { out[b + u] = run; run += v[u]; }
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (g < s1) out[g] = run + x - v;
+    run += __shfl_sync(0xffffffffu, x, 31);
   }
   if (threadIdx.x == 0) out[n] = tot;
 }
@@ -1317,12 +1334,6 @@ __device__ __forceinline__ size_t idx3(int Ng, int a, int b, int c) {
   return ((size_t) a * Ng + b) * Ng + c;
 }
 
-__device__ __forceinline__ real norm_paint(const real *q, const real *rho,
-    size_t c) {
-  const real r = rho[c];
-  return (r > (real) EZ_REAL_TOL) ? q[c] / r : q[c];
-}
-
 __global__ void __launch_bounds__(NT)
 vel_kernel(const real *__restrict__ rho, const real *__restrict__ q0,
     const real *__restrict__ q1, const real *__restrict__ q2, int Ng, real igs,
@@ -1348,22 +1359,32 @@ vel_kernel(const real *__restrict__ rho, const real *__restrict__ q0,
     const real wa[8] = {wx0, wx0, wx0, wx0, wx1, wx1, wx1, wx1};
     const real wb[8] = {wy0, wy0, wy1, wy1, wy0, wy0, wy1, wy1};
     const real wc[8] = {wz0, wz1, wz0, wz1, wz0, wz1, wz0, wz1};
+    // all 32 gathers issued before any of them is used
+    const real *qs[3] = {q0, q1, q2};
+    real rv[8], qv[3][8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) rv[c] = rho[cs[c]];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int c = 0; c < 8; c++) qv[d][c] = qs[d][cs[c]];
     real rw[8];
     real rs = 0;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
-      rw[c] = rho[cs[c]] * wa[c] * wb[c] * wc[c];
+      rw[c] = rv[c] * wa[c] * wb[c] * wc[c];
       rs = (c == 0) ? rw[0] : rs + rw[c];
     }
     const double fac = vfac / rs;
     real *outs[3] = {vx, vy, vz};
-    const real *qs[3] = {q0, q1, q2};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       real v = 0;
 #pragma unroll
       for (int c = 0; c < 8; c++) {
-        const real pr = norm_paint(qs[d], rho, cs[c]) * rw[c];
+        // the painted momentum per unit density (pop_tracer.c:681)
+        const real np = (rv[c] > (real) EZ_REAL_TOL) ? qv[d][c] / rv[c] : qv[d][c];
+        const real pr = np * rw[c];
         v = (c == 0) ? pr : v + pr;
       }
       outs[d][t] = v * fac;
