@@ -526,11 +526,16 @@ constexpr int WK = 8;                        // columns per tile (passes I, J)
 // keeps two (measured faster at 1024^3 despite small spills).
 template <int E> constexpr int wpass_min_blocks() { return E >= 32 ? 1 : 2; }
 
+#ifndef EZ_PASSI_WK
+#define EZ_PASSI_WK 8
+#endif
+constexpr int WKI = EZ_PASSI_WK;              // pass I: columns per tile = warps per block
 template <int E>
-__global__ void __launch_bounds__(32 * WNW, 2)
+__global__ void __launch_bounds__(32 * WKI, 16 / WKI)
 wpass_i(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0,
     int Ng, int Nkp, const cplx *__restrict__ twn) {
   constexpr int n = 32 * E, LS = n + 1;
+  constexpr int WK = WKI, WNW = WKI;
   extern __shared__ unsigned char smraw[];
   cplx *tw = (cplx *) smraw;
   cplx *b0 = tw + n;                         // WK lines: S, then A_0
@@ -1143,11 +1148,11 @@ template <int E>
 int run_wpass_i(EzMesh *m, const FftPlanDev &pn) {
   const int Ng = m->Ng;
   const size_t n = 32 * E, LS = n + 1;
-  const size_t sm_i = sizeof(cplx) * (n + 2 * WK * LS);
+  const size_t sm_i = sizeof(cplx) * (n + 2 * WKI * LS);
   cudaFuncSetAttribute(wpass_i<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_i);
-  const int nkt = (m->Nk + WK - 1) / WK;
+  const int nkt = (m->Nk + WKI - 1) / WKI;
   ez_stage_begin(m, ST_FFT_I);
-  wpass_i<E><<<dim3(nkt, Ng), 32 * WNW, sm_i, m->stream>>>(m->spec[0], m->spec[1],
+  wpass_i<E><<<dim3(nkt, Ng), 32 * WKI, sm_i, m->stream>>>(m->spec[0], m->spec[1],
       m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
   ez_stage_end(m, ST_FFT_I);
   return 0;
