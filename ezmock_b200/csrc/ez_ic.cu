@@ -136,7 +136,7 @@ __device__ __forceinline__ float twice_u_f(int ran, uint32_t x) {
 }
 #endif
 
-// One block per (i, j) row of the half-complex grid.  The generator (RAN),
+// One warp per (i, j) row of the half-complex grid.  The generator (RAN),
 // the draws per cell (PER: 2, or 1 with fixed amplitudes) and the inverted
 // phase (IPH) are template parameters; a row's draws and output are
 // addressed from per-row pointers, and the two draws of a cell come as one
@@ -192,8 +192,12 @@ ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
     const double *__restrict__ pkq, const float *__restrict__ pka, int logpk, int Ng,
     int Nk, int Nkp, double kfac, double Pfac) {
   const int Ngh = Ng >> 1;
-  const int row = blockIdx.x;                       // i * Ng + j
-  const int i = row / Ng, j = row - i * Ng;
+  // one warp per row: the row's set-up is shared by the 8 cells (512^3) a
+  // lane computes (with a block per row it was about half of the kernel's
+  // instructions)
+  const int i = blockIdx.y, j = blockIdx.x * (IC_NT / 32) + (threadIdx.x >> 5);
+  if (j >= Ng) return;
+  const int row = i * Ng + j;
   const int ki = (i <= Ngh) ? i : i - Ng;
   const int kj = (j <= Ngh) ? j : j - Ng;
   const int ni = (i == 0) ? 0 : Ng - i, nj = (j == 0) ? 0 : Ng - j;
@@ -206,7 +210,7 @@ ic_kernel(cplx *__restrict__ S, const uint32_t *__restrict__ draws,
   // draws of cell c = row * Nk + k (c >= 1) start at (c - 1) PER
   const size_t rowc = (size_t) row * Nk, prowc = ((size_t) ni * Ng + nj) * Nk;
   cplx *Srow = S + (size_t) row * Nkp;
-  for (int k = threadIdx.x; k < Nkp; k += IC_NT) {
+  for (int k = threadIdx.x & 31; k < Nkp; k += 32) {
     cplx out;
     out.x = 0; out.y = 0;
     if (k < Nk && (row | k) != 0) {
@@ -291,7 +295,8 @@ int ez_ic_spectrum(EzMesh *m, const EzPk *pk, double Lbox, int ran,
              : (fixamp ? ic_kernel<0, 1, true> : ic_kernel<0, 2, true>))
       : (ran ? (fixamp ? ic_kernel<1, 1, false> : ic_kernel<1, 2, false>)
              : (fixamp ? ic_kernel<0, 1, false> : ic_kernel<0, 2, false>));
-  kern<<<(unsigned) ((size_t) Ng * Ng), IC_NT, 0, m->stream>>>(
+  kern<<<dim3((unsigned) ((Ng + IC_NT / 32 - 1) / (IC_NT / 32)), (unsigned) Ng), IC_NT, 0,
+      m->stream>>>(
       m->spec[0], draws, m->pkq, (const float *) (m->pkq + nq), pk->log ? 1 : 0, Ng, m->Nk,
       m->Nkp, kfac, Pfac); ez_count_launch();
   ez_stage_end(m, ST_IC);

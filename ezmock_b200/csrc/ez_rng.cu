@@ -463,22 +463,19 @@ mt_jumpd_kernel(uint32_t *states, const MtJumpArgs a, int nst, int nseg,
 // Block c generates draws [c*L, min((c+1)*L, count)) from window states[c]
 // through a 2048-word ring: a round computes the 454 words 624+g .. 1077+g,
 // which depend only on words g .. 623+g, as two steps of 227 (see the loop
-// below).  Every word is stored twice, at i mod 2048 and 2048 + i mod 2048,
-// so that reads at i .. i + 397 never wrap.
+// below).  Reads wrap with a mask (storing every word twice instead, so that
+// no read wraps, costs two shared stores per word where the mask costs one
+// AND, and the kernel is bound by its shared-memory traffic).
 constexpr int R_THREADS = 256;
 __global__ void __launch_bounds__(R_THREADS)
 mt_ring_kernel(const uint32_t *__restrict__ states, uint64_t L, uint64_t count,
     uint32_t *__restrict__ out) {
-  __shared__ uint32_t ring[4096];
+  __shared__ uint32_t ring[2048];
   const int t = threadIdx.x;
   const uint64_t c0 = (uint64_t) blockIdx.x * L;
   if (c0 >= count) return;
   const uint64_t n = (count - c0 < L) ? count - c0 : L;
-  for (int k = t; k < MT_N; k += R_THREADS) {
-    const uint32_t v = states[(size_t) blockIdx.x * MT_N + k];
-    ring[k] = v;
-    ring[k + 2048] = v;
-  }
+  for (int k = t; k < MT_N; k += R_THREADS) ring[k] = states[(size_t) blockIdx.x * MT_N + k];
   __syncthreads();
   // Step one of a round: x[b + 624] from x[b], x[b + 1], x[b + 397] for
   // b = g + t; step two: x[b + 851] from x[b + 227], x[b + 228] and
@@ -486,29 +483,27 @@ mt_ring_kernel(const uint32_t *__restrict__ states, uint64_t L, uint64_t count,
   // [g, g + 624) and writes [g + 624, g + 1078); the words it overwrites,
   // [g - 1424, g - 970) mod 2048, are no longer needed.
   constexpr int S = MT_N - MT_M;
+  constexpr uint32_t W = 2047;
   uint32_t *o = out + c0 + t;
   uint32_t p = (uint32_t) t;                     // (g + t) mod 2048
   const uint64_t nfull = n / (2 * S);
   for (uint64_t r = 0; r < nfull; r++) {
     if (t < S) {
-      const uint32_t y = mt_f(ring[p], ring[p + 1], ring[p + MT_M]);
-      const uint32_t y2 = mt_f(ring[p + S], ring[p + S + 1], y);
-      const uint32_t q = (p + MT_N) & 2047, q2 = (p + MT_N + S) & 2047;
-      ring[q] = y;
-      ring[q + 2048] = y;
-      ring[q2] = y2;
-      ring[q2 + 2048] = y2;
+      const uint32_t y = mt_f(ring[p], ring[(p + 1) & W], ring[(p + MT_M) & W]);
+      const uint32_t y2 = mt_f(ring[(p + S) & W], ring[(p + S + 1) & W], y);
+      ring[(p + MT_N) & W] = y;
+      ring[(p + MT_N + S) & W] = y2;
       o[0] = mt_temper(y);
       o[S] = mt_temper(y2);
     }
     o += 2 * S;
-    p = (p + 2 * S) & 2047;
+    p = (p + 2 * S) & W;
     __syncthreads();
   }
   const uint64_t rem = n - nfull * (2 * S);      // the last, partial round
   if (rem && t < S) {
-    const uint32_t y = mt_f(ring[p], ring[p + 1], ring[p + MT_M]);
-    const uint32_t y2 = mt_f(ring[p + S], ring[p + S + 1], y);
+    const uint32_t y = mt_f(ring[p], ring[(p + 1) & W], ring[(p + MT_M) & W]);
+    const uint32_t y2 = mt_f(ring[(p + S) & W], ring[(p + S + 1) & W], y);
     if ((uint64_t) t < rem) o[0] = mt_temper(y);
     if ((uint64_t) (S + t) < rem) o[S] = mt_temper(y2);
   }
