@@ -300,17 +300,17 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
     skey_t *__restrict__ keys, unsigned long long *counter, skey_t *__restrict__ cand,
     uint16_t *__restrict__ cidx, size_t ccap, unsigned long long *__restrict__ cstart,
     unsigned int *__restrict__ ccnt) {
-  // candidates are written warp row by warp row (ballot ranks), so each
-  // warp's stores are contiguous; their order within the chunk's range is
-  // irrelevant (the keys are sorted, the copies carry their place)
+  // candidates are written in cell order within the chunk's range (an
+  // exclusive scan of the (row, warp) ballot counts), so that emission can
+  // walk them in the order of the tracers
   constexpr int NW = NT / 32;
-  __shared__ unsigned int wtot[NW];
+  __shared__ unsigned int pre[ROWS * NW];
+  __shared__ unsigned int wsum[ROWS * NW / 32];
   __shared__ unsigned long long sbase;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const size_t b0 = (size_t) blockIdx.x * CH;
   real v[ROWS];
   unsigned int bal[ROWS];
-  unsigned int wc = 0;
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {               // all loads first
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
@@ -320,31 +320,45 @@ compact_kernel(const real *__restrict__ rhot, size_t N, real thres,
   for (int q = 0; q < ROWS; q++) {
     const size_t id = b0 + (size_t) q * NT + threadIdx.x;
     bal[q] = __ballot_sync(0xffffffffu, id < N && !(v[q] < thres));
-    wc += __popc(bal[q]);
-  }
-  if (lane == 0) wtot[w] = wc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long tot = 0;
-    for (int k = 0; k < NW; k++) tot += wtot[k];
-    sbase = tot ? atomicAdd(counter, tot) : 0;
-    cstart[blockIdx.x] = sbase;
-    ccnt[blockIdx.x] = (unsigned int) tot;
+    if (lane == 0) pre[q * NW + w] = __popc(bal[q]);
   }
   __syncthreads();
-  unsigned long long off = sbase;
-  for (int k = 0; k < w; k++) off += wtot[k];
+  static_assert(ROWS * NW <= 32 * 32, "scan width");
+  unsigned int c = 0, incl = 0;
+  if (threadIdx.x < ROWS * NW) {
+    c = pre[threadIdx.x];
+    incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[w] = incl;
+  }
+  __syncthreads();
+  if (threadIdx.x < ROWS * NW) {
+    unsigned int base = 0;
+    for (int k = 0; k < w; k++) base += wsum[k];
+    pre[threadIdx.x] = base + incl - c;
+    if (threadIdx.x == ROWS * NW - 1) {
+      const unsigned long long tot = base + incl;
+      sbase = tot ? atomicAdd(counter, tot) : 0;
+      cstart[blockIdx.x] = sbase;
+      ccnt[blockIdx.x] = (unsigned int) tot;
+    }
+  }
+  __syncthreads();
+  const unsigned long long off = sbase;
   const unsigned int lt = (1u << lane) - 1;
 #pragma unroll
   for (int q = 0; q < ROWS; q++) {
     if ((bal[q] >> lane) & 1) {
-      const unsigned long long pos = off + __popc(bal[q] & lt);
+      const unsigned long long pos = off + pre[q * NW + w] + __popc(bal[q] & lt);
       const skey_t k = to_key(v[q]);
       keys[pos] = k;
       // a second copy with the cell's place in the chunk, kept for emission
       if (pos < ccap) { cand[pos] = k; cidx[pos] = (uint16_t) (q * NT + threadIdx.x); }
     }
-    off += __popc(bal[q]);
   }
 }
 
@@ -791,27 +805,28 @@ __device__ __forceinline__ int cell_count(real v, const real *lo, const int *ntr
 
 // Tracers of a chunk from its candidates (the cells at or above the
 // selection's cut, listed by compact_kernel): only they can hold tracers.
+// One warp per chunk, eight chunks per block.
+constexpr int CW = NT / 32;                      // chunks per block (emission)
+
 __global__ void __launch_bounds__(NT)
 cand_count_kernel(const skey_t *__restrict__ cand,
     const unsigned long long *__restrict__ cstart, const unsigned int *__restrict__ ccnt,
-    const BoundOut *__restrict__ bo, unsigned long long *cnt) {
+    const BoundOut *__restrict__ bo, unsigned long long *cnt, size_t nblk) {
   __shared__ real slo[EZ_MAX_NT];
   __shared__ int sntr[EZ_MAX_NT];
-  __shared__ unsigned long long sw[32];
-  const unsigned int n = ccnt[blockIdx.x];
-  if (!n) {
-    if (threadIdx.x == 0) cnt[blockIdx.x] = 0;
-    return;
-  }
   const int nb = bo->nbins;
   for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
   __syncthreads();
-  const skey_t *c = cand + cstart[blockIdx.x];
+  const int lane = threadIdx.x & 31;
+  const size_t ch = (size_t) blockIdx.x * CW + (threadIdx.x >> 5);
+  if (ch >= nblk) return;
+  const unsigned int n = ccnt[ch];
+  const skey_t *c = cand + cstart[ch];
   unsigned long long t = 0;
-  for (unsigned int i = threadIdx.x; i < n; i += NT) t += cell_count(from_key(c[i]), slo, sntr, nb);
-  unsigned long long tot;
-  block_scan<unsigned long long>(t, &tot, sw);
-  if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
+  for (unsigned int i = lane; i < n; i += 32) t += cell_count(from_key(c[i]), slo, sntr, nb);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (lane == 0) cnt[ch] = t;
 }
 
 __global__ void __launch_bounds__(NT)
@@ -929,10 +944,9 @@ tracer_cell_kernel(const real *__restrict__ rhot, size_t N,
   }
 }
 
-// Tracer cells from the selection's candidates only: a chunk's candidates
-// mark their places in a 4096-bit map; one thread per 32-cell word sums the
-// counts of its marked cells, a scan over the 128 words gives each word's
-// first tracer, and the thread then writes its cells' indices in cell order
+// Tracer cells from the selection's candidates only: compact_kernel lists a
+// chunk's candidates in cell order, so one warp per chunk walks them 32 at a
+// time, and a warp scan of their counts gives each candidate's first tracer
 // (the same order and offsets as tracer_cell_kernel, which walks every cell
 // of the chunk).
 template <typename cid_t>
@@ -940,50 +954,34 @@ __global__ void __launch_bounds__(NT)
 tracer_cell_cand_kernel(const BoundOut *__restrict__ bo, const unsigned long long *__restrict__ off,
     unsigned long long ntr, cid_t *__restrict__ cid, const skey_t *__restrict__ cand,
     const uint16_t *__restrict__ cidx, const unsigned long long *__restrict__ cstart,
-    const unsigned int *__restrict__ ccnt) {
-  constexpr int NWD = CH / 32;                  // map words
-  static_assert(NWD <= NT && NWD % 32 == 0, "one thread per map word");
+    const unsigned int *__restrict__ ccnt, size_t nblk) {
   __shared__ real slo[EZ_MAX_NT];
   __shared__ int sntr[EZ_MAX_NT];
-  __shared__ uint16_t lcnt[CH];
-  __shared__ unsigned int bmp[NWD];
-  __shared__ unsigned int wtot[NWD / 32];
-  const unsigned int nc = ccnt[blockIdx.x];
-  if (!nc) return;
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int nb = bo->nbins;
-  for (int e = t; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
-  if (t < NWD) bmp[t] = 0;
+  for (int e = threadIdx.x; e < nb; e += NT) { slo[e] = bo->lo[e]; sntr[e] = bo->ntr[e]; }
   __syncthreads();
-  const unsigned long long c0 = cstart[blockIdx.x];
-  for (unsigned int i = t; i < nc; i += NT) {
-    const int p = cidx[c0 + i];
-    lcnt[p] = (uint16_t) cell_count(from_key(cand[c0 + i]), slo, sntr, nb);
-    atomicOr(&bmp[p >> 5], 1u << (p & 31));
-  }
-  __syncthreads();
-  unsigned int bits = 0, mine = 0;
-  if (t < NWD) {
-    bits = bmp[t];
-    for (unsigned int b = bits; b; b &= b - 1) mine += lcnt[t * 32 + __ffs(b) - 1];
-  }
-  unsigned int incl = mine;
+  const int lane = threadIdx.x & 31;
+  const size_t ch = (size_t) blockIdx.x * CW + (threadIdx.x >> 5);
+  if (ch >= nblk) return;
+  const unsigned int n = ccnt[ch];
+  const unsigned long long c0 = cstart[ch];
+  const size_t b0 = ch * CH;
+  unsigned long long tt = off[ch];
+  for (unsigned int i0 = 0; i0 < n; i0 += 32) {
+    const unsigned int i = i0 + lane;
+    const int k = (i < n) ? cell_count(from_key(cand[c0 + i]), slo, sntr, nb) : 0;
+    unsigned int incl = (unsigned int) k;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  if (t < NWD && lane == 31) wtot[w] = incl;
-  __syncthreads();
-  if (t >= NWD) return;
-  unsigned int base = 0;
-  for (int k = 0; k < w; k++) base += wtot[k];
-  unsigned long long tt = off[blockIdx.x] + base + incl - mine;
-  const size_t b0 = (size_t) blockIdx.x * CH;
-  for (unsigned int b = bits; b; b &= b - 1) {
-    const int p = t * 32 + __ffs(b) - 1;
-    const cid_t id = (cid_t) (b0 + p);
-    for (int m = 0; m < (int) lcnt[p] && tt < ntr; m++, tt++) cid[tt] = id;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (k) {
+      const cid_t id = (cid_t) (b0 + cidx[c0 + i]);
+      unsigned long long t = tt + incl - (unsigned int) k;
+      for (int m = 0; m < k && t < ntr; m++, t++) cid[t] = id;
+    }
+    tt += __shfl_sync(0xffffffffu, incl, 31);
   }
 }
 
@@ -1847,7 +1845,8 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   // changed them (then the remaining counts are in nt16)
   const bool usecand = !nt16 && cb.ok;
   if (usecand)
-    cand_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(cb.key, ps.cstart, ps.ccnt, bo, bcnt);
+    cand_count_kernel<<<(unsigned) ((nblk + CW - 1) / CW), NT, 0, st>>>(cb.key, ps.cstart,
+        ps.ccnt, bo, bcnt, nblk);
   else
     tracer_count_kernel<<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bcnt, nt16);
   ez_count_launch();
@@ -1863,17 +1862,18 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
   void *cidv = (N <= 0xffffffffULL) ? (void *) (cvx + iv) : (void *) cvx;
   if (N <= 0xffffffffULL) {
     if (usecand)
-      tracer_cell_cand_kernel<uint32_t><<<(unsigned) nblk, NT, 0, st>>>(bo, bscan,
-          (unsigned long long) nrand, (uint32_t *) cidv, cb.key, cb.idx, ps.cstart, ps.ccnt);
+      tracer_cell_cand_kernel<uint32_t><<<(unsigned) ((nblk + CW - 1) / CW), NT, 0, st>>>(bo,
+          bscan, (unsigned long long) nrand, (uint32_t *) cidv, cb.key, cb.idx, ps.cstart,
+          ps.ccnt, nblk);
     else
       tracer_cell_kernel<uint32_t><<<(unsigned) nblk, NT, 0, st>>>(rhot, N, bo, bscan,
           (unsigned long long) nrand, (uint32_t *) cidv, nt16);
   }
   else {                                            // vx and vy (iv = 0)
     if (usecand)
-      tracer_cell_cand_kernel<unsigned long long><<<(unsigned) nblk, NT, 0, st>>>(bo, bscan,
-          (unsigned long long) nrand, (unsigned long long *) cidv, cb.key, cb.idx, ps.cstart,
-          ps.ccnt);
+      tracer_cell_cand_kernel<unsigned long long><<<(unsigned) ((nblk + CW - 1) / CW), NT, 0,
+          st>>>(bo, bscan, (unsigned long long) nrand, (unsigned long long *) cidv, cb.key,
+          cb.idx, ps.cstart, ps.ccnt, nblk);
     else
       tracer_cell_kernel<unsigned long long><<<(unsigned) nblk, NT, 0, st>>>(rhot, N,
           bo, bscan, (unsigned long long) nrand, (unsigned long long *) cidv, nt16);
