@@ -1143,14 +1143,87 @@ bool run_tpass_j(EzMesh *m, const FftPlanDev &pn) {
   return EZ_CUDA_OK(cudaGetLastError());
 }
 
+// pass I with row-major tiles of 8 columns (the 64-byte-swizzled layout of
+// the TMA pass J, so a warp reading one column meets each bank at most
+// twice), copied in 16-byte chunks (two columns of a row) and stored as
+// 16-byte chunks, half the copy instructions of wpass_i; a per-warp scratch
+// line for the transforms.  The same transforms, so the same results.
+template <int E>
+__global__ void __launch_bounds__(32 * WKI, 2)
+wpass_i_rm(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__ A0,
+    int Ng, int Nkp, const cplx *__restrict__ twn) {
+  static_assert(WKI == 8, "one warp per column of an 8-column tile");
+  constexpr int n = 32 * E;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx *tw = (cplx *) smraw;                 // n
+  cplx *b0 = tw + n;                         // n x 8: S, then A_0
+  cplx *b1 = b0 + 8 * n;                     // n x 8: A_x
+  cplx *scr = b1 + 8 * n;                    // a scratch line per warp
+  const int j = blockIdx.y, k0 = blockIdx.x * 8;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
+  const size_t pst = (size_t) Ng * Nkp;
+  const cplx *src = S + (size_t) j * Nkp + k0;
+#pragma unroll 4
+  for (int q = threadIdx.x; q < n * 4; q += 32 * WKI) {
+    const int row = q >> 2, c = (q & 3) << 1;
+    __pipeline_memcpy_async(b0 + tix(row, c), src + row * pst + c, 16);
+  }
+  __pipeline_commit();
+  __pipeline_wait_prior(0);
+  __syncthreads();
+  const int c = w;
+  cplx *line = scr + (size_t) w * n;
+  cplx v[E];
+#pragma unroll
+  for (int m = 0; m < E; m++) {
+    const int i = 32 * m + lane;
+    v[m] = b0[tix(i, c)];
+    const rt f = freq_of(i, Ng);
+    v[m].x *= f;
+    v[m].y *= f;
+  }
+  line_fft<E, 1, use_t<E>(0)>(v, tw, lane, line);
+#pragma unroll
+  for (int q = 0; q < E; q++) b1[tix(line_out<E, use_t<E>(0)>(lane, q), c)] = v[q];
+#pragma unroll
+  for (int m = 0; m < E; m++) v[m] = b0[tix(32 * m + lane, c)];
+  __syncwarp();
+  line_fft<E, 1, use_t<E>(0)>(v, tw, lane, line);
+#pragma unroll
+  for (int q = 0; q < E; q++) b0[tix(line_out<E, use_t<E>(0)>(lane, q), c)] = v[q];
+  __syncthreads();
+  cplx *dx = Ax + (size_t) j * Nkp + k0, *d0 = A0 + (size_t) j * Nkp + k0;
+#pragma unroll 4
+  for (int q = threadIdx.x; q < n * 4; q += 32 * WKI) {
+    const int row = q >> 2, c2 = (q & 3) << 1;
+    const size_t g = row * pst + c2;
+    *reinterpret_cast<float4 *>(dx + g) = *reinterpret_cast<const float4 *>(b1 + tix(row, c2));
+    *reinterpret_cast<float4 *>(d0 + g) = *reinterpret_cast<const float4 *>(b0 + tix(row, c2));
+  }
+}
+
 template <int E>
 int run_wpass_i(EzMesh *m, const FftPlanDev &pn) {
   const int Ng = m->Ng;
   const size_t n = 32 * E, LS = n + 1;
-  const size_t sm_i = sizeof(cplx) * (n + 2 * WKI * LS);
-  cudaFuncSetAttribute(wpass_i<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_i);
   const int nkt = (m->Nk + WKI - 1) / WKI;
   ez_stage_begin(m, ST_FFT_I);
+#ifdef SINGLE_PREC
+  // 512^3 (E = 16): 0.739 -> 0.713 ms with the row-major tiles; at 256^3 they
+  // measured slower (0.094 -> 0.145 ms: fewer blocks per SM) and at 1024^3
+  // the same
+  if constexpr (E == 16) {
+    const size_t sm_r = sizeof(cplx) * (n + 16 * n + WKI * n);
+    cudaFuncSetAttribute(wpass_i_rm<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_r);
+    wpass_i_rm<E><<<dim3(nkt, Ng), 32 * WKI, sm_r, m->stream>>>(m->spec[0], m->spec[1],
+        m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
+    ez_stage_end(m, ST_FFT_I);
+    return 0;
+  }
+#endif
+  const size_t sm_i = sizeof(cplx) * (n + 2 * WKI * LS);
+  cudaFuncSetAttribute(wpass_i<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_i);
   wpass_i<E><<<dim3(nkt, Ng), 32 * WKI, sm_i, m->stream>>>(m->spec[0], m->spec[1],
       m->spec[2], Ng, m->Nkp, pn.tw); ez_count_launch();
   ez_stage_end(m, ST_FFT_I);
