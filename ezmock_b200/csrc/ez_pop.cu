@@ -252,10 +252,10 @@ bias_kernel(const real *__restrict__ rho, real *__restrict__ rhot, size_t N,
           st[pos] = t;
           bin = logb_bin(t);
         }
-        // one shared atomic per distinct bin of the warp (a ballot per bin
-        // between the warp's lowest and highest bin measured 1.8x slower)
-        const unsigned int grp = __match_any_sync(0xffffffffu, bin);
-        if (mine && lane == __ffs(grp) - 1) atomicAdd(&sh[bin], (unsigned int) __popc(grp));
+        // one shared atomic per rank (at 512^3: 1.18 -> 1.11 ms for the stage
+        // against one per distinct bin of the warp through __match_any_sync,
+        // and 2.06 ms with a ballot per bin between the warp's extremes)
+        if (mine) atomicAdd(&sh[bin], 1u);
       }
     }
   }
