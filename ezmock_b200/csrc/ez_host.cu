@@ -415,6 +415,7 @@ EZMOCK *EZmock_init(const double Lbox, const int Ngrid, const int randgen,
   EzMesh *m = MESH(ez);
   m->device = -1;
   m->fft_tma = true;
+  m->fft_tma_i = true;
   m->sel_path = -1;
   return ez;
 }
@@ -1021,6 +1022,10 @@ int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     case EZMOCKB200_OPT_FFT_TMA:
       if (value != 0 && value != 1) return (*err = EZMOCK_ERR_ARG_PARAMS);
       m->fft_tma = value == 1;
+      return 0;
+    case EZMOCKB200_OPT_FFT_TMA_I:
+      if (value != 0 && value != 1) return (*err = EZMOCK_ERR_ARG_PARAMS);
+      m->fft_tma_i = value == 1;
       return 0;
     case EZMOCKB200_OPT_SELECT_SORT:
       if (value != 0 && value != 1) return (*err = EZMOCK_ERR_ARG_PARAMS);

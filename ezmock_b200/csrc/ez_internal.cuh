@@ -87,6 +87,7 @@ struct EzMesh {
   bool cic_oh_set;         // cic_oh set by the caller for the next field
   bool cic_legacy;         // FP32 CIC on 16 x 16 tiles instead of 16 x 32
   bool fft_tma;            // FP32 FFT passes I and J through TMA-staged tiles
+  bool fft_tma_i;           // FP32 FFT pass I through TMA-staged tiles (with fft_tma)
   bool sel_sort;           // selection boundaries from a full radix sort
   int sel_path;            // last selection: 0 buckets, 1 sort, 2 buckets then sort
 

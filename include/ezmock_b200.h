@@ -48,6 +48,11 @@ extern "C" {
    counts; the first falls back to the second by itself when the buckets at
    the boundaries hold too many candidates. */
 #define EZMOCKB200_OPT_SELECT_SORT 9
+/* FP32 transform of the initial field along x, while EZMOCKB200_OPT_FFT_TMA
+   is 1: 1 (default) moves its tiles with the Tensor Memory Accelerator on
+   grids of 512^3 and 1024^3, 0 with per-thread asynchronous copies.
+   Both give the same field bit for bit. */
+#define EZMOCKB200_OPT_FFT_TMA_I 10
 
 int EZmockB200_set_option(EZMOCK *ez, const int option, const long value,
     int *err);

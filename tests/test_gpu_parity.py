@@ -213,6 +213,26 @@ def test_fft_tma_matches_cp_async(pk_table, Ng, L):
             assert relmax(out[0][d], psi[d]) <= 5e-6
 
 
+@pytest.mark.parametrize("Ng,L", [(512, 2500.0), (1024, 5000.0)])
+def test_fft_pass_i_tma_bit_identical(pk_table, Ng, L):
+    """The FP32 transform along x with its tiles moved by the Tensor Memory
+    Accelerator (the default) and by per-thread cp.async copies runs the same
+    line transforms, so the displacement fields agree bit for bit (1024^3:
+    psi_x, the field whose pass-I output is the separate A_x spectrum, and
+    psi_z)."""
+    k, P = pk_table
+    comps = (0, 2) if Ng >= 1024 else (0, 1, 2)
+    out = []
+    for tma in (1, 0):
+        m = make(32, Ng, L, 1, 13, k, P)
+        m.set_option(10, tma)
+        m.create_dens_field_from_ic()
+        out.append([m.field(d) for d in comps])
+        del m
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("rng", [0, 1])
 def test_golden_reference_fp64(golden, pk_table, rng):
     """16^3 fields, counts and catalogue of the reference's own build."""
