@@ -724,8 +724,11 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
   if (run_populate(ez, params, nexp, att_part, &n, err)) return *err;
   if (!m->cpy || !EZ_CUDA_OK(cudaEventRecord(m->ev_cat, m->stream)))
     return (*err = EZMOCK_ERR_UNKNOWN);
+  // host threads of the copy-out: on the GPU boxes (16 cores) a 75 MB
+  // pinned-to-malloc copy took 1.86 ms with 8 threads (slower than its
+  // 1.40 ms DMA) and 1.08 ms with 16; more threads than cores were slower
   int nthr = CONF(ez)->nthread > 0 ? CONF(ez)->nthread : omp_get_num_procs();
-  nthr = std::max(1, std::min(nthr, 8));
+  nthr = std::max(1, std::min(nthr, 16));
   const size_t bytes_arr = n * sizeof(real);
   const bool pooled = m->hpool_mib >= 0 && bytes_arr >= ((size_t) 4 << 20);
   if (pooled && !m->hpool) m->hpool = new HostPool(nthr);
@@ -757,7 +760,8 @@ int EZmock_populate_tracer(EZMOCK *ez, const real *params, const size_t nexp,
   // the velocities.  (512^3, 75 MB: the copy-out after the GPU work took
   // 2.26 ms with two 8 MB buffers and four threads, 1.85 with three, 1.49
   // with three and six threads, 1.18 with three 16 MB buffers and eight
-  // threads; 32 MB pieces or four buffers no better.)
+  // threads; 32 MB pieces or four buffers no better; 1.08 with sixteen
+  // threads, against 1.1-1.6 for 4 or 8 MB pieces in four to eight buffers.)
   ez_stage_begin(m, ST_D2H);
   const size_t piece = (size_t) 16 << 20;
   constexpr int NB = 3;
