@@ -1207,37 +1207,47 @@ wpass_i_rm(const cplx *__restrict__ S, cplx *__restrict__ Ax, cplx *__restrict__
 // Pass I with its tiles moved by the Tensor Memory Accelerator (FP32): one
 // CTA per tile, the transforms of wpass_i_rm (so the results are the same
 // bit for bit), but the S tile arrives by tensor copies of 256-row boxes
-// (16 floats x 1 j x 256 i of the spectrum, 64-byte swizzle: the smem
-// layout is that of tix) and A_x and A_0 leave the same way, so the
-// load/store unit only carries the transforms' own shared-memory traffic
-// (pass I is bound by that unit: its cp.async fills and 16-byte
-// shared-to-global copies were a third of it).  Thread 0 issues the copies;
+// (2 KC floats x 1 j x 256 i of the spectrum, swizzled) and A_x and A_0
+// leave the same way, so the load/store unit only carries the transforms'
+// own shared-memory traffic, not the cp.async fills and the 16-byte
+// shared-to-global copies of wpass_i_rm.  Thread 0 issues the copies;
 // the mbarrier wait is bounded, and a wait that runs out sets
 // stats->tma_err (read by the population), skips the tile and lets the
 // copies land before the CTA returns.
-template <int E> constexpr int tpi_min_blocks() { return E == 16 ? 2 : 1; }
-template <int E> struct TpiLayout {
+// KC columns per tile (one warp each): 8 (64-byte rows, 64-byte swizzle, the
+// layout of tix) or 4 (32-byte rows, 32-byte swizzle: the 16-byte half of a
+// row is flipped by bit 2 of the row).
+template <int KC>
+__device__ __forceinline__ int tixk(int row, int c) {
+  if constexpr (KC == 8) return tix(row, c);
+  else return row * 4 + ((((c >> 1) ^ ((row >> 2) & 1)) << 1) | (c & 1));
+}
+template <int E, int KC> constexpr int tpi_min_blocks() {
+  return KC == 4 ? (E == 16 ? 4 : 2) : (E == 16 ? 2 : 1);
+}
+template <int E, int KC> struct TpiLayout {
   static constexpr int n = 32 * E;
-  static constexpr size_t tile = (size_t) n * 64;
+  static constexpr size_t tile = (size_t) n * KC * 8;
   static constexpr size_t tw_bytes = ((size_t) n * 8 + 1023) / 1024 * 1024;
   static constexpr bool T = use_t<E>(0);
-  static constexpr size_t scr_bytes = T ? (size_t) 8 * n * 8 : 0;
+  static constexpr size_t scr_bytes = T ? (size_t) KC * n * 8 : 0;
   // [twiddles][tile S -> A_0][tile A_x][scratch lines][barrier] + alignment
   static constexpr size_t bytes = tw_bytes + 2 * tile + scr_bytes + 64 + 1024;
 };
 
-template <int E>
-__global__ void __launch_bounds__(256, tpi_min_blocks<E>())
+template <int E, int KC>
+__global__ void __launch_bounds__(32 * KC, (tpi_min_blocks<E, KC>()))
 tpass_i_tile(const __grid_constant__ CUtensorMap ms, const __grid_constant__ CUtensorMap mx,
     const __grid_constant__ CUtensorMap m0, int Ng, int nkt, const cplx *__restrict__ twn,
     EzCicStats *stats) {
-  typedef TpiLayout<E> Lay;
+  typedef TpiLayout<E, KC> Lay;
   constexpr int n = Lay::n;
   constexpr int NB = n / TP_BOX > 0 ? n / TP_BOX : 1;   // boxes per tile
   constexpr int BR = n < TP_BOX ? n : TP_BOX;           // rows per box
+  constexpr int RB = KC * 8;                            // bytes per row
   extern __shared__ __align__(1024) unsigned char tpi_raw[];
-  // 1 KB alignment of the tiles (the swizzle pattern repeats every 512 B),
-  // kept as an offset into the shared array so addresses stay 32-bit
+  // 1 KB alignment of the tiles (the swizzle patterns repeat every 256 or
+  // 512 B), kept as an offset into the shared array so addresses stay 32-bit
   unsigned char *base = tpi_raw + ((1024u - (ez_smem_addr(tpi_raw) & 1023u)) & 1023u);
   cplx *tw = (cplx *) base;
   cplx *b0 = (cplx *) (base + Lay::tw_bytes);              // S, then A_0
@@ -1253,7 +1263,8 @@ tpass_i_tile(const __grid_constant__ CUtensorMap ms, const __grid_constant__ CUt
     ez_mbar_expect_tx(full, (uint32_t) Lay::tile);
 #pragma unroll
     for (int b = 0; b < NB; b++)
-      ez_tma_load3((unsigned char *) b0 + (size_t) b * BR * 64, &ms, 16 * kt, j, b * BR, full);
+      ez_tma_load3((unsigned char *) b0 + (size_t) b * BR * RB, &ms, 2 * KC * kt, j, b * BR,
+                   full);
   }
   for (int e = threadIdx.x; e < n; e += blockDim.x) tw[e] = twn[e];
   __syncthreads();
@@ -1265,20 +1276,20 @@ tpass_i_tile(const __grid_constant__ CUtensorMap ms, const __grid_constant__ CUt
 #pragma unroll
     for (int m = 0; m < E; m++) {
       const int i = 32 * m + lane;
-      v[m] = b0[tix(i, c)];
+      v[m] = b0[tixk<KC>(i, c)];
       const rt f = freq_of(i, Ng);
       v[m].x *= f;
       v[m].y *= f;
     }
     line_fft<E, 1, Lay::T>(v, tw, lane, line);
 #pragma unroll
-    for (int q = 0; q < E; q++) b1[tix(line_out<E, Lay::T>(lane, q), c)] = v[q];
+    for (int q = 0; q < E; q++) b1[tixk<KC>(line_out<E, Lay::T>(lane, q), c)] = v[q];
 #pragma unroll
-    for (int m = 0; m < E; m++) v[m] = b0[tix(32 * m + lane, c)];
+    for (int m = 0; m < E; m++) v[m] = b0[tixk<KC>(32 * m + lane, c)];
     __syncwarp();
     line_fft<E, 1, Lay::T>(v, tw, lane, line);
 #pragma unroll
-    for (int q = 0; q < E; q++) b0[tix(line_out<E, Lay::T>(lane, q), c)] = v[q];
+    for (int q = 0; q < E; q++) b0[tixk<KC>(line_out<E, Lay::T>(lane, q), c)] = v[q];
   }
   ez_fence_async_smem();
   const bool all = __syncthreads_and(ok);
@@ -1287,9 +1298,9 @@ tpass_i_tile(const __grid_constant__ CUtensorMap ms, const __grid_constant__ CUt
       const int j = blockIdx.x / nkt, kt = blockIdx.x - j * nkt;
 #pragma unroll
       for (int b = 0; b < NB; b++) {
-        const size_t off = (size_t) b * BR * 64;
-        ez_tma_store3(&mx, 16 * kt, j, b * BR, (const unsigned char *) b1 + off);
-        ez_tma_store3(&m0, 16 * kt, j, b * BR, (const unsigned char *) b0 + off);
+        const size_t off = (size_t) b * BR * RB;
+        ez_tma_store3(&mx, 2 * KC * kt, j, b * BR, (const unsigned char *) b1 + off);
+        ez_tma_store3(&m0, 2 * KC * kt, j, b * BR, (const unsigned char *) b0 + off);
       }
       ez_tma_commit();
       ez_tma_wait_read<0>();                 // the tiles are read before the CTA ends
@@ -1303,40 +1314,41 @@ tpass_i_tile(const __grid_constant__ CUtensorMap ms, const __grid_constant__ CUt
 // Pass I through tpass_i_tile (FP32, Ng = 32 E with E = 16 or 32).  False if
 // nothing was launched (no tensor maps or shared memory): the cp.async
 // kernels run then.
-template <int E>
+template <int E, int KC>
 bool run_tpass_i(EzMesh *m, const FftPlanDev &pn) {
   const int Ng = m->Ng;
   if (sizeof(rt) != 4 || 32 * E != Ng || E < 16 || E > 32) return false;
   const uint64_t dims[3] = {2 * (uint64_t) m->Nkp, (uint64_t) Ng, (uint64_t) Ng};
   const uint64_t str[2] = {2 * (uint64_t) m->Nkp * sizeof(rt),
                            2 * (uint64_t) m->Nkp * Ng * sizeof(rt)};
-  const uint32_t box[3] = {16, 1, (uint32_t) std::min(Ng, TP_BOX)};
+  const uint32_t box[3] = {2 * KC, 1, (uint32_t) std::min(Ng, TP_BOX)};
   CUtensorMap mp[3];
   for (int a = 0; a < 3; a++)
     if (!ez_tma_encode(&mp[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, m->spec[a], dims, str, box,
-                       CU_TENSOR_MAP_SWIZZLE_64B))
+                       KC == 8 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B))
       return false;
-  const size_t sm = TpiLayout<E>::bytes;
-  if (!EZ_CUDA_OK(cudaFuncSetAttribute(tpass_i_tile<E>,
+  const size_t sm = TpiLayout<E, KC>::bytes;
+  if (!EZ_CUDA_OK(cudaFuncSetAttribute(tpass_i_tile<E, KC>,
           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm))) {
     cudaGetLastError();
     return false;
   }
-  const int nkt = (m->Nk + 7) / 8;
+  const int nkt = (m->Nk + KC - 1) / KC;
   ez_stage_begin(m, ST_FFT_I);
-  tpass_i_tile<E><<<(unsigned) (Ng * nkt), 256, sm, m->stream>>>(mp[0], mp[1], mp[2], Ng, nkt,
-      pn.tw, (EzCicStats *) m->stats); ez_count_launch();
+  tpass_i_tile<E, KC><<<(unsigned) (Ng * nkt), 32 * KC, sm, m->stream>>>(mp[0], mp[1], mp[2],
+      Ng, nkt, pn.tw, (EzCicStats *) m->stats); ez_count_launch();
   ez_stage_end(m, ST_FFT_I);
   return EZ_CUDA_OK(cudaGetLastError());
 }
 
 template <int E>
 int run_wpass_i(EzMesh *m, const FftPlanDev &pn) {
-  // 512^3: 0.720 -> 0.638 ms, 1024^3: 5.73 -> 5.09 ms with the tensor
-  // copies; at 256^3 the column-major tiles of wpass_i stay faster (0.095
-  // against 0.132 ms)
+  // With the tensor copies: 512^3 0.720 -> 0.643 ms on 8-column tiles, 0.613
+  // on 4-column tiles (four CTAs of four warps per SM); 1024^3 5.73 -> 5.02
+  // ms on 8-column tiles (8.64 on 4-column ones).  At 256^3 the column-major
+  // tiles of wpass_i stay faster (0.095 against 0.132 ms).
   if constexpr (E >= 16) {
-    if (m->fft_tma && m->fft_tma_i && run_tpass_i<E>(m, pn)) return 0;
+    if (m->fft_tma && m->fft_tma_i && run_tpass_i<E, E == 16 ? 4 : 8>(m, pn)) return 0;
   }
   const int Ng = m->Ng;
   const size_t n = 32 * E, LS = n + 1;
