@@ -334,7 +334,7 @@ __device__ __forceinline__ void red_add(uint32_t addr, int v) {
 template <int OH>
 __global__ void __launch_bounds__(TNT, 1)
 cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
-    const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
+    const real *__restrict__ p2, real *rho, float4 *pq,
     int Ng, real igs, CicStats *stats, unsigned int *list, int nzs) {
   constexpr int OWX = TX + 2 * OH + 1;        // Lagrangian columns along x
   constexpr int OWY = TY + 2 * OH + 1;        // and along y
@@ -474,24 +474,46 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
         }
       }
     }
-    // slices 8p-8 .. 8p-1 are final: written if the CTA owns them (a sector
-    // of eight slices per cell and quantity) and cleared
+    // slices 8p-8 .. 8p-1 are final: written if the CTA owns them and
+    // cleared.  First the density of each cell's eight slices (one 32-byte
+    // sector of rho per thread), then one (slice pair, cell) per thread,
+    // cells fastest: the four quantities of two slices go out as two float4
+    // of the interleaved grid (q0, q1, q2, rho per cell: one sector) and the
+    // ring slots are cleared.
     __syncthreads();
     const int zo = (p - 1) * TZ;
     const bool wr = zo >= zs && zo < ze;
-    for (int t = threadIdx.x; t < 4 * TSLOT; t += TNT) {
-      const int q = t / TSLOT, cc = t - q * TSLOT;
-      int *src = tring + q * TQS + rbase * TSLOT + cc;
-      int v[TZ];
+    const float fr = 1.f / RHO_SCALE;
+    if (wr) {
+      for (int cc = threadIdx.x; cc < TSLOT; cc += TNT) {
+        const int *src = tring + rbase * TSLOT + cc;
+        int v[TZ];
 #pragma unroll
-      for (int kk = 0; kk < TZ; kk++) { v[kk] = src[kk * TSLOT]; src[kk * TSLOT] = 0; }
-      if (wr) {
-        const float f = (q == 0) ? (1.f / RHO_SCALE) : minv;
-        real *g = (q == 0) ? rho : (q == 1) ? q0 : (q == 2) ? q1 : q2;
+        for (int kk = 0; kk < TZ; kk++) v[kk] = src[kk * TSLOT];
         const int cx = cc / TY, cy = cc - (cc / TY) * TY;
-        float4 *dst = reinterpret_cast<float4 *>(g + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo);
-        dst[0] = make_float4(v[0] * f, v[1] * f, v[2] * f, v[3] * f);
-        dst[1] = make_float4(v[4] * f, v[5] * f, v[6] * f, v[7] * f);
+        float4 *dst = reinterpret_cast<float4 *>(
+            rho + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo);
+        dst[0] = make_float4(v[0] * fr, v[1] * fr, v[2] * fr, v[3] * fr);
+        dst[1] = make_float4(v[4] * fr, v[5] * fr, v[6] * fr, v[7] * fr);
+      }
+      __syncthreads();
+    }
+    for (int t = threadIdx.x; t < (TZ / 2) * TSLOT; t += TNT) {
+      const int sp = t / TSLOT, cc = t - sp * TSLOT;
+      int v[4][2];
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          int *src = tring + q * TQS + (rbase + 2 * sp + h) * TSLOT + cc;
+          v[q][h] = *src;
+          *src = 0;
+        }
+      if (wr) {
+        const int cx = cc / TY, cy = cc - (cc / TY) * TY;
+        const size_t g = ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo + 2 * sp;
+        pq[g] = make_float4(v[1][0] * minv, v[2][0] * minv, v[3][0] * minv, v[0][0] * fr);
+        pq[g + 1] = make_float4(v[1][1] * minv, v[2][1] * minv, v[3][1] * minv, v[0][1] * fr);
       }
     }
     __syncthreads();
@@ -502,10 +524,13 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
   if ((threadIdx.x & 31) == 0 && nfar2) atomicAdd(&stats->nfar2, nfar2);
 }
 
-// Deposits the listed far-displaced particles with global atomics.
+// Deposits the listed far-displaced particles with global atomics, into rho
+// and the separate painted grids q0..q2, or (IL) into rho and the
+// interleaved grid pq = (q0, q1, q2, rho) per cell.
+template <bool IL>
 __global__ void __launch_bounds__(CIC_NT)
 fixup_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
-    const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2,
+    const real *__restrict__ p2, real *rho, real *q0, real *q1, real *q2, real *pq,
     int Ng, real igs, const CicStats *stats, const unsigned int *list) {
   const unsigned int n = stats->nlist;
   for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < n;
@@ -529,10 +554,18 @@ fixup_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
 #pragma unroll
         for (int cz = 0; cz < 2; cz++) {
           const size_t g = idx3(Ng, xs[a], ys[b], zs[cz]);
-          atomicAdd(rho + g, wxs[a] * wys[b] * wzs[cz]);
-          atomicAdd(q0 + g, (wxs[a] * pv[0]) * wys[b] * wzs[cz]);
-          atomicAdd(q1 + g, (wxs[a] * pv[1]) * wys[b] * wzs[cz]);
-          atomicAdd(q2 + g, (wxs[a] * pv[2]) * wys[b] * wzs[cz]);
+          const real w = wxs[a] * wys[b] * wzs[cz];
+          atomicAdd(rho + g, w);
+          if (IL) {
+            atomicAdd(pq + 4 * g, (wxs[a] * pv[0]) * wys[b] * wzs[cz]);
+            atomicAdd(pq + 4 * g + 1, (wxs[a] * pv[1]) * wys[b] * wzs[cz]);
+            atomicAdd(pq + 4 * g + 2, (wxs[a] * pv[2]) * wys[b] * wzs[cz]);
+            atomicAdd(pq + 4 * g + 3, w);
+          } else {
+            atomicAdd(q0 + g, (wxs[a] * pv[0]) * wys[b] * wzs[cz]);
+            atomicAdd(q1 + g, (wxs[a] * pv[1]) * wys[b] * wzs[cz]);
+            atomicAdd(q2 + g, (wxs[a] * pv[2]) * wys[b] * wzs[cz]);
+          }
         }
   }
 }
@@ -599,6 +632,7 @@ int ez_cic(EzMesh *m, double Lbox) {
   const unsigned grid = (unsigned) ((N + CIC_NT - 1) / CIC_NT < 148u * 64u
       ? (N + CIC_NT - 1) / CIC_NT : 148u * 64u);
   ez_stage_begin(m, ST_CIC);
+  m->paint_il = false;                       // set by the 16 x 32 tile assignment
   if (m->cic_mode == 1) {
     // 4 x N 64-bit accumulators, allocated on first use
     const size_t need = 4 * N * sizeof(unsigned long long);
@@ -658,15 +692,18 @@ int ez_cic(EzMesh *m, double Lbox) {
           if (cost < best * 0.999) { best = cost; nzs = s; }
         }
         const unsigned nblk = (unsigned) (tiles * nzs);
+        float4 *pq = reinterpret_cast<float4 *>(m->pq);
         if (m->cic_oh != 2)
           cic_tile_kernel<3><<<nblk, TNT, TSMEM, m->stream>>>(m->psi[0], m->psi[1],
-              m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list, nzs);
+              m->psi[2], m->rho, pq, Ng, igs, stats, list, nzs);
         else
           cic_tile_kernel<2><<<nblk, TNT, TSMEM, m->stream>>>(m->psi[0], m->psi[1],
-              m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list, nzs);
+              m->psi[2], m->rho, pq, Ng, igs, stats, list, nzs);
+        m->paint_il = true;
       }
       else {
         const unsigned nblk = (unsigned) ((Ng / OT) * (Ng / OT));
+        m->paint_il = false;
         if (m->cic_oh != 2)
           cic_owner_kernel<3><<<nblk, OWN_NT, smem, m->stream>>>(m->psi[0], m->psi[1],
               m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
@@ -675,9 +712,15 @@ int ez_cic(EzMesh *m, double Lbox) {
               m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs, stats, list);
       }
       ez_count_launch();
-      fixup_kernel<<<148 * 4, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
-          m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], Ng, igs,
-          stats, list); ez_count_launch();
+      if (m->paint_il)
+        fixup_kernel<true><<<148 * 4, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
+            m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], m->pq, Ng, igs,
+            stats, list);
+      else
+        fixup_kernel<false><<<148 * 4, CIC_NT, 0, m->stream>>>(m->psi[0], m->psi[1],
+            m->psi[2], m->rho, m->paint[0], m->paint[1], m->paint[2], m->pq, Ng, igs,
+            stats, list);
+      ez_count_launch();
       // this field's count of particles beyond 2 cells, for the next field's
       // halo (2 only while almost none move farther; those take the
       // global-atomic fixup); read into pinned memory without waiting

@@ -349,7 +349,7 @@ int ez_mesh_alloc(EzMesh *m, int Ng) {
   if (!EZ_CUDA_OK(cudaMalloc(&spec, 3 * m->Nspec * sizeof(cplx))) ||
       !EZ_CUDA_OK(cudaMalloc(&psi, 3 * m->N * sizeof(real))) ||
       !EZ_CUDA_OK(cudaMalloc(&m->rho, m->N * sizeof(real))) ||
-      !EZ_CUDA_OK(cudaMalloc(&paint, 3 * m->N * sizeof(real))) ||
+      !EZ_CUDA_OK(cudaMalloc(&paint, (sizeof(real) == 4 ? 4 : 3) * m->N * sizeof(real))) ||
       !EZ_CUDA_OK(cudaMalloc(&m->draws, ndraw * sizeof(uint32_t)))) {
     if (spec) cudaFree(spec);
     if (psi) cudaFree(psi);
@@ -369,6 +369,7 @@ int ez_mesh_alloc(EzMesh *m, int Ng) {
     m->psi[d] = psi + d * m->N;
     m->paint[d] = paint + d * m->N;
   }
+  m->pq = paint;
   return 0;
 }
 
@@ -1071,6 +1072,15 @@ int EZmockB200_copy_field(EZMOCK *ez, const int which, real *out, int *err) {
   else if (which >= 4 && which < 7) src = m->paint[which - 4];
   else return (*err = EZMOCK_ERR_ARG_PARAMS);
   cudaSetDevice(m->device);
+  if (which >= 4 && m->paint_il) {
+    // the interleaved grids: component which - 4 of each cell's four values
+    // (a strided copy; this accessor is for tests and inspection)
+    if (!EZ_CUDA_OK(cudaMemcpy2DAsync(out, sizeof(real), m->pq + (which - 4), 4 * sizeof(real),
+            sizeof(real), m->N, cudaMemcpyDeviceToHost, m->stream)) ||
+        !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
+      return (*err = EZMOCK_ERR_UNKNOWN);
+    return 0;
+  }
   if (!EZ_CUDA_OK(cudaMemcpyAsync(out, src, m->N * sizeof(real), cudaMemcpyDeviceToHost, m->stream)) ||
       !EZ_CUDA_OK(cudaStreamSynchronize(m->stream)))
     return (*err = EZMOCK_ERR_UNKNOWN);

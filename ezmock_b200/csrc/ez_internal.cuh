@@ -98,6 +98,11 @@ struct EzMesh {
   real *psi[3];
   real *rho;
   real *paint[3];          // CIC of psi_d (un-normalised momenta)
+  // (FP32) the same grids interleaved with the density, (q0, q1, q2, rho) per
+  // cell in 4 N reals (the block that holds paint[]), written instead of
+  // paint[] by the 16 x 32 tile assignment when paint_il is set
+  real *pq;
+  bool paint_il;
   cplx *spec[3];
   uint32_t *draws;
   size_t draws_cap;

@@ -1333,9 +1333,16 @@ __device__ __forceinline__ size_t idx3(int Ng, int a, int b, int c) {
   return ((size_t) a * Ng + b) * Ng + c;
 }
 
+// Velocity of each tracer from the painted grids at its eight CIC cells
+// (pop_tracer.c:593-683 painting, :697-753 interpolation).  IL: the grids interleaved with the density,
+// (q0, q1, q2, rho) per cell, one 16-byte load per cell instead of four
+// 4-byte loads from four grids (a tracer's eight cells touch 4 to 8 sectors
+// instead of 16 to 32).
+template <bool IL>
 __global__ void __launch_bounds__(NT)
 vel_kernel(const real *__restrict__ rho, const real *__restrict__ q0,
-    const real *__restrict__ q1, const real *__restrict__ q2, int Ng, real igs,
+    const real *__restrict__ q1, const real *__restrict__ q2, const real *__restrict__ pq,
+    int Ng, real igs,
     double vfac, size_t n, const real *__restrict__ x, const real *__restrict__ y,
     const real *__restrict__ z, real *vx, real *vy, real *vz) {
   for (size_t t = (size_t) blockIdx.x * blockDim.x + threadIdx.x; t < n;
@@ -1361,12 +1368,25 @@ vel_kernel(const real *__restrict__ rho, const real *__restrict__ q0,
     // all 32 gathers issued before any of them is used
     const real *qs[3] = {q0, q1, q2};
     real rv[8], qv[3][8];
+    if constexpr (IL) {
+#ifdef SINGLE_PREC
 #pragma unroll
-    for (int c = 0; c < 8; c++) rv[c] = rho[cs[c]];
+      for (int c = 0; c < 8; c++) {
+        const float4 a = reinterpret_cast<const float4 *>(pq)[cs[c]];
+        qv[0][c] = a.x;
+        qv[1][c] = a.y;
+        qv[2][c] = a.z;
+        rv[c] = a.w;
+      }
+#endif
+    } else {
 #pragma unroll
-    for (int d = 0; d < 3; d++)
+      for (int c = 0; c < 8; c++) rv[c] = rho[cs[c]];
 #pragma unroll
-      for (int c = 0; c < 8; c++) qv[d][c] = qs[d][cs[c]];
+      for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int c = 0; c < 8; c++) qv[d][c] = qs[d][cs[c]];
+    }
     real rw[8];
     real rs = 0;
 #pragma unroll
@@ -1897,10 +1917,17 @@ int ez_populate(EzMesh *m, int Ng, double Lbox, int ran, uint64_t seed,
 
   // ---- 5./6. velocities and dispersion ----
   ez_stage_begin(m, ST_VEL);
-  if (nrand)
-    vel_kernel<<<grid_for(nrand, NT), NT, 0, st>>>(m->rho, m->paint[0],
-        m->paint[1], m->paint[2], Ng, igs, vfac, nrand, cx + iv, cy + iv, cz + iv, cvx + iv,
-        cvy + iv, cvz + iv); ez_count_launch();
+  if (nrand) {
+    if (m->paint_il)
+      vel_kernel<true><<<grid_for(nrand, NT), NT, 0, st>>>(m->rho, m->paint[0],
+          m->paint[1], m->paint[2], m->pq, Ng, igs, vfac, nrand, cx + iv, cy + iv, cz + iv,
+          cvx + iv, cvy + iv, cvz + iv);
+    else
+      vel_kernel<false><<<grid_for(nrand, NT), NT, 0, st>>>(m->rho, m->paint[0],
+          m->paint[1], m->paint[2], m->pq, Ng, igs, vfac, nrand, cx + iv, cy + iv, cz + iv,
+          cvx + iv, cvy + iv, cvz + iv);
+    ez_count_launch();
+  }
   const size_t nd_disp = 6 * ((nt_all + 1) / 2);
   if ((e = ensure_draws(m, std::max(nd_disp, (size_t) 1)))) return e;
   const uint32_t *ddisp = nullptr;
