@@ -331,6 +331,24 @@ __device__ __forceinline__ void red_add(uint32_t addr, int v) {
   asm volatile("red.shared.add.s32 [%0], %1;" :: "r"(addr), "r"(v) : "memory");
 }
 
+// 32-byte global accesses (one sector, 32-byte aligned) as single 256-bit
+// instructions: the lanes of a warp touch 32 different sectors here (one per
+// Lagrangian column or output cell), so each access instruction costs a
+// load/store-unit pass per sector, and one 256-bit access instead of two
+// 128-bit ones halves those passes.
+__device__ __forceinline__ void ld8(const float *p, float4 &a, float4 &b) {
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z),
+                 "=f"(b.w)
+               : "l"(p));
+}
+__device__ __forceinline__ void st8(float *p, float4 a, float4 b) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
+               :: "l"(p), "f"(a.x), "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z),
+                  "f"(b.w)
+               : "memory");
+}
+
 template <int OH>
 __global__ void __launch_bounds__(TNT, 1)
 cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
@@ -386,10 +404,7 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
     const size_t o = ((size_t) C.iw * Ng + C.jw) * Ng + zwrap(p);
     const real *src[3] = {p0 + o, p1 + o, p2 + o};
 #pragma unroll
-    for (int a = 0; a < 3; a++) {
-      cur[k][a][0] = *reinterpret_cast<const float4 *>(src[a]);
-      cur[k][a][1] = *reinterpret_cast<const float4 *>(src[a] + 4);
-    }
+    for (int a = 0; a < 3; a++) ld8(src[a], cur[k][a][0], cur[k][a][1]);
   };
 #pragma unroll
   for (int k = 0; k < 2; k++)
@@ -491,10 +506,9 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
 #pragma unroll
         for (int kk = 0; kk < TZ; kk++) v[kk] = src[kk * TSLOT];
         const int cx = cc / TY, cy = cc - (cc / TY) * TY;
-        float4 *dst = reinterpret_cast<float4 *>(
-            rho + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo);
-        dst[0] = make_float4(v[0] * fr, v[1] * fr, v[2] * fr, v[3] * fr);
-        dst[1] = make_float4(v[4] * fr, v[5] * fr, v[6] * fr, v[7] * fr);
+        st8(rho + ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo,
+            make_float4(v[0] * fr, v[1] * fr, v[2] * fr, v[3] * fr),
+            make_float4(v[4] * fr, v[5] * fr, v[6] * fr, v[7] * fr));
       }
       __syncthreads();
     }
@@ -512,8 +526,9 @@ cic_tile_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
       if (wr) {
         const int cx = cc / TY, cy = cc - (cc / TY) * TY;
         const size_t g = ((size_t) (i0 + cx) * Ng + (j0 + cy)) * Ng + zo + 2 * sp;
-        pq[g] = make_float4(v[1][0] * minv, v[2][0] * minv, v[3][0] * minv, v[0][0] * fr);
-        pq[g + 1] = make_float4(v[1][1] * minv, v[2][1] * minv, v[3][1] * minv, v[0][1] * fr);
+        st8(reinterpret_cast<float *>(pq + g),
+            make_float4(v[1][0] * minv, v[2][0] * minv, v[3][0] * minv, v[0][0] * fr),
+            make_float4(v[1][1] * minv, v[2][1] * minv, v[3][1] * minv, v[0][1] * fr));
       }
     }
     __syncthreads();
