@@ -301,7 +301,7 @@ cic_owner_kernel(const real *__restrict__ p0, const real *__restrict__ p1,
 // and walks it eight slices at a time.  Each thread owns two of the
 // (16 + 2 OH + 1) x (32 + 2 OH + 1) Lagrangian columns whose particles can
 // reach the tile, for the whole walk.  A column's next eight particles (one
-// 32-byte sector per displacement field, two 16-byte loads) are loaded into
+// 32-byte sector per displacement field, a 256-bit load) are loaded into
 // registers while its current eight are deposited, so every sector is read
 // from memory once.  Accumulation is 32-bit fixed point (rho in units of
 // 2^-21, the momenta in units of 2^-s from max |psi|, as in the kernel above)
