@@ -183,3 +183,26 @@ def test_python_wrapper_interface(pk_table):
     m.eval_growth_params(0.8, 0.31)
     with pytest.raises(RuntimeError, match="k range insufficient"):
         m.setup_linear_pk(pk_table[0][500:], pk_table[1][500:])
+
+
+def test_extension_options():
+    """EZmockB200_set_option (include/ezmock_b200.h) accepts each option's
+    documented values and rejects the others with the sticky argument error,
+    on the host (no GPU work)."""
+    from ezmock_b200 import EZmock
+    valid = {1: [0, 1], 2: [0, 1], 3: [0, 1], 4: [1, 12345], 5: [2, 3], 6: [0, 64, 2048],
+             7: [16, 32], 8: [0, 1], 9: [0, 1], 10: [0, 1]}
+    invalid = {3: [-1], 4: [0, -5], 5: [1, 4], 6: [-1], 7: [8, 64], 8: [2, -1], 9: [2],
+               10: [2, -1], 11: [0], 0: [0]}
+    for opt, vals in valid.items():
+        m = EZmock(Lbox=200.0, Ngrid=16)
+        for v in vals:
+            m.set_option(opt, v)
+    for opt, vals in invalid.items():
+        for v in vals:
+            m = EZmock(Lbox=200.0, Ngrid=16)
+            with pytest.raises(RuntimeError):
+                m.set_option(opt, v)
+            # the error is sticky: a valid call afterwards still fails
+            with pytest.raises(RuntimeError):
+                m.set_option(2, 0)
